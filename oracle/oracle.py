@@ -1,0 +1,228 @@
+"""ctypes access to the CPU oracle -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only as the checker.  It also reads and writes the "series
+bundle" fixture container described in oracle/series_bundle.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import struct
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libodba_oracle.so")
+
+NIL, DIAGONAL, RIGHT, UP, OPEN_RIGHT, NIL_OPEN_RIGHT = 255, 1, 2, 3, 4, 5
+MOVE_NAMES = {DIAGONAL: "DIAG", RIGHT: "RIGHT", UP: "UP", OPEN_RIGHT: "OPEN_RIGHT",
+              NIL: "NIL", NIL_OPEN_RIGHT: "NIL_OPEN_RIGHT"}
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        for sfx in ("f32", "f64"):
+            f = getattr(_lib, f"oracle_dtw_pair_{sfx}")
+            f.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, P, P]
+            f.restype = ctypes.c_int
+            f = getattr(_lib, f"oracle_pairwise_{sfx}")
+            f.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P,
+                          ctypes.c_int64, ctypes.c_int]
+            f.restype = ctypes.c_int
+            f = getattr(_lib, f"oracle_medoid_{sfx}")
+            f.argtypes = [P, ctypes.c_int, P, P]
+            f.restype = ctypes.c_int
+            f = getattr(_lib, f"oracle_dba_update_{sfx}")
+            f.argtypes = [P, ctypes.c_size_t, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, P, P, P]
+            f.restype = ctypes.c_double
+            f = getattr(_lib, f"oracle_path_triples_{sfx}")
+            f.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, P, ctypes.c_int64]
+            f.restype = ctypes.c_int64
+            f = getattr(_lib, f"oracle_znorm_{sfx}")
+            f.argtypes = [P, P, P, ctypes.c_int, P, P]
+            f.restype = ctypes.c_int
+    return _lib
+
+
+def _sfx(dtype) -> str:
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def pack(series: list[np.ndarray], dtype=None):
+    """Concatenate a ragged list; returns (flat, offsets, lens) as numpy arrays."""
+    dtype = np.dtype(dtype or series[0].dtype)
+    lens = np.array([len(s) for s in series], dtype=np.uint64)
+    offsets = np.zeros(len(series), dtype=np.uint64)
+    if len(series) > 1:
+        offsets[1:] = np.cumsum(lens)[:-1]
+    flat = np.concatenate([np.asarray(s, dtype=dtype) for s in series]) if series else \
+        np.zeros(0, dtype)
+    return np.ascontiguousarray(flat), offsets, lens
+
+
+def dtw_pair(first, second, open_start=0, open_end=0, fma_mode=1, with_path=False):
+    first = np.ascontiguousarray(first)
+    second = np.ascontiguousarray(second, dtype=first.dtype)
+    d = np.zeros(1, dtype=first.dtype)
+    path = np.zeros(len(first) * len(second), dtype=np.uint8) if with_path else None
+    rc = getattr(lib(), f"oracle_dtw_pair_{_sfx(first.dtype)}")(
+        _ptr(first), len(first), _ptr(second), len(second), open_start, open_end, fma_mode,
+        _ptr(d), _ptr(path) if with_path else None)
+    assert rc == 0
+    if with_path:
+        return d[0], path.reshape(len(first), len(second))
+    return d[0]
+
+
+def pairwise(series, open_start=0, open_end=0, fma_mode=1, pair_list=None, threads=0):
+    flat, offsets, lens = pack(series)
+    n = len(series)
+    out = np.zeros(n * (n - 1) // 2, dtype=flat.dtype)
+    pl = None if pair_list is None else np.ascontiguousarray(pair_list, dtype=np.int64)
+    rc = getattr(lib(), f"oracle_pairwise_{_sfx(flat.dtype)}")(
+        _ptr(flat), _ptr(offsets), _ptr(lens), n, open_start, open_end, fma_mode, _ptr(out),
+        _ptr(pl) if pl is not None else None, 0 if pl is None else len(pl), threads)
+    assert rc == 0
+    return out
+
+
+def medoid(dists, lens):
+    dists = np.ascontiguousarray(dists)
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    n = len(lens)
+    sos = np.zeros(n, dtype=dists.dtype)
+    m = getattr(lib(), f"oracle_medoid_{_sfx(dists.dtype)}")(_ptr(dists), n, _ptr(lens), _ptr(sos))
+    return m, sos
+
+
+def dba_update(centroid, members, open_start=0, open_end=0, fma_mode=1):
+    centroid = np.ascontiguousarray(centroid)
+    flat, offsets, lens = pack(members, centroid.dtype)
+    Lc = len(centroid)
+    mean = np.zeros(Lc, dtype=centroid.dtype)
+    counts = np.zeros(Lc, dtype=np.uint32)
+    sums = np.zeros(Lc, dtype=centroid.dtype)
+    delta = getattr(lib(), f"oracle_dba_update_{_sfx(centroid.dtype)}")(
+        _ptr(centroid), Lc, _ptr(flat), _ptr(offsets), _ptr(lens), len(members), open_start,
+        open_end, fma_mode, _ptr(mean), _ptr(counts), _ptr(sums))
+    return mean, counts, sums, delta
+
+
+def path_triples(centroid, seq, open_start=0, open_end=0, fma_mode=1):
+    centroid = np.ascontiguousarray(centroid)
+    seq = np.ascontiguousarray(seq, dtype=centroid.dtype)
+    cap = len(centroid) + len(seq) + 2
+    tri = np.zeros(3 * cap, dtype=np.int64)
+    k = getattr(lib(), f"oracle_path_triples_{_sfx(centroid.dtype)}")(
+        _ptr(centroid), len(centroid), _ptr(seq), len(seq), open_start, open_end, fma_mode,
+        _ptr(tri), cap)
+    assert k >= 0
+    return tri[:3 * k].reshape(k, 3)
+
+
+def znorm(series):
+    flat, offsets, lens = pack(series)
+    n = len(series)
+    means = np.zeros(n)
+    sigmas = np.zeros(n)
+    getattr(lib(), f"oracle_znorm_{_sfx(flat.dtype)}")(_ptr(flat), _ptr(offsets), _ptr(lens), n,
+                                                        _ptr(means), _ptr(sigmas))
+    out = [flat[int(o):int(o) + int(L)].copy() for o, L in zip(offsets, lens)]
+    return out, means, sigmas
+
+
+# ---- series bundle I/O (layout in oracle/series_bundle.h) ----
+
+def write_bundle(path: str, series: list[np.ndarray], dtype=None) -> None:
+    dtype = np.dtype(dtype or (series[0].dtype if series else np.float32))
+    with open(path, "wb") as f:
+        f.write(b"ODBS")
+        f.write(struct.pack("<IQ", dtype.itemsize, len(series)))
+        f.write(np.array([len(s) for s in series], dtype="<u8").tobytes())
+        for s in series:
+            f.write(np.ascontiguousarray(s, dtype=dtype).tobytes())
+
+
+def read_bundle(path: str) -> list[np.ndarray]:
+    with open(path, "rb") as f:
+        raw = f.read()
+    assert raw[:4] == b"ODBS", path
+    esize, n = struct.unpack_from("<IQ", raw, 4)
+    lens = np.frombuffer(raw, dtype="<u8", count=n, offset=16)
+    dtype = np.float64 if esize == 8 else np.float32
+    pos = 16 + 8 * n
+    out = []
+    for L in lens:
+        L = int(L)
+        out.append(np.frombuffer(raw, dtype=dtype, count=L, offset=pos).copy())
+        pos += L * esize
+    return out
+
+
+def perform_dba(series, open_start=0, open_end=0, norm=1, fma_mode=1, max_rounds=250):
+    """CPU restatement of performDBA for one cluster (cdist == 1), dba.hpp:863-1189.
+
+    Returns a dict with the sorted order, the medoid index (in sorted order),
+    the pair distances, the final centroid (rescaled when norm), the number of
+    rounds run and each round's delta."""
+    dtype = series[0].dtype
+    tmax = np.finfo(dtype).max
+    work = []
+    for s in series:
+        s = np.array(s, dtype=dtype)
+        if s[-1] >= np.sqrt(tmax):  # dba.hpp:868-872
+            s = s[:-1]
+        work.append(s)
+    order = sorted(range(len(work)), key=lambda i: len(work[i]))  # stable, dba.hpp:882-883
+    work = [work[i] for i in order]
+    means = sigmas = None
+    if norm:
+        work, means, sigmas = znorm(work)
+    dists = pairwise(work, open_start, open_end, fma_mode)
+    lens = np.array([len(s) for s in work], dtype=np.uint64)
+    med, _ = medoid(dists, lens)
+    centroid = work[med].copy()
+    prev = two_prev = np.zeros_like(centroid)
+    deltas = []
+    new = centroid
+    rounds = 0
+    for i in range(max_rounds):
+        new, _, _, delta = dba_update(centroid, work, open_start, open_end, fma_mode)
+        rounds += 1
+        deltas.append(delta)
+        if delta == 0:
+            break
+        if open_start or open_end:
+            if i >= 1 and new.tobytes() == two_prev.tobytes():
+                break
+            if i > 1:
+                two_prev = prev.copy()
+            if i > 0:
+                prev = new.copy()
+        centroid = new
+    out = new.copy()
+    if norm:
+        out = (np.float64(means[med]) + out.astype(np.float64) * np.float64(sigmas[med])).astype(dtype)
+    return {"order": order, "medoid": med, "dists": dists, "centroid": out, "rounds": rounds,
+            "deltas": deltas, "means": means, "sigmas": sigmas}

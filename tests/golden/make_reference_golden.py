@@ -1,0 +1,205 @@
+"""Generate golden fixtures by running the reference's own GPU build.
+
+Test infrastructure.  Runs oracle/_ref/ref_harness (the reference's sources
+compiled for sm_100a by oracle/Makefile) on seeded inputs and stores its
+outputs under an output directory (default gpurun_out/golden_ref).  The
+committed copy lives in tests/golden/ref/; tests compare the CUDA path and
+the CPU oracle against it.
+
+Run on a B200 box from the repository root:
+    python tests/golden/make_reference_golden.py [out_dir]
+"""
+from __future__ import annotations
+
+import glob
+import gzip
+import json
+import os
+import shutil
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import oracle as O  # noqa: E402
+from opendba_b200 import synth  # noqa: E402
+
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+MODES = {"global": (0, 0), "open_start": (1, 0), "open_end": (0, 1), "open": (1, 1)}
+FIXTURES = "tests/golden/ref_fixtures"
+
+
+def run(args, log, cwd=None):
+    t0 = time.time()
+    p = subprocess.run([HARNESS] + [str(a) for a in args], capture_output=True, text=True, cwd=cwd)
+    log.write(json.dumps({"args": [str(a) for a in args], "rc": p.returncode,
+                          "secs": round(time.time() - t0, 3), "stdout": p.stdout[-2000:],
+                          "stderr": p.stderr[-2000:]}) + "\n")
+    log.flush()
+    return p
+
+
+def mix_series(dtype, seed):
+    """Lengths that hit the swath edges (1024, 2048), tiny series and odd sizes; unsorted."""
+    lens = [2, 3, 7, 33, 100, 511, 1023, 1024, 1025, 1500, 2047, 2048, 2049, 2500, 3100,
+            700, 1200, 64, 1030, 2000]
+    rng = np.random.default_rng(seed)
+    out = []
+    for i, L in enumerate(lens):
+        if i % 2:
+            x = np.cumsum(rng.standard_normal(L))
+        else:
+            x = synth.step_signal(rng, L, 90.0, 12.0, 10.0, 2.0)
+        sd = x.std()
+        out.append(((x - x.mean()) / (sd if sd else 1.0)).astype(dtype))
+    return out
+
+
+def paths_to_npz(prefix, dst):
+    files = sorted(glob.glob(prefix + ".path*.txt"),
+                   key=lambda f: int(f.rsplit(".path", 1)[1].split(".")[0]))
+    arrays = {}
+    for f in files:
+        k = int(f.rsplit(".path", 1)[1].split(".")[0])
+        rows = []
+        with open(f) as fh:
+            fh.readline()
+            for line in fh:
+                a = line.rstrip("\n").split("\t")
+                rows.append((int(a[0]), int(a[2]), a[4]))
+        names = {v: k2 for k2, v in O.MOVE_NAMES.items()}
+        arrays[f"ij{k}"] = np.array([(r[0], r[1]) for r in rows], dtype=np.int32)
+        arrays[f"mv{k}"] = np.array([names.get(r[2], 0) for r in rows], dtype=np.uint8)
+    np.savez_compressed(dst, **arrays)
+
+
+def gz(src, dst):
+    with open(src, "rb") as f, gzip.open(dst, "wb", compresslevel=9) as g:
+        g.write(f.read())
+
+
+def main():
+    out = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden_ref"))
+    os.makedirs(out, exist_ok=True)
+    tmp = os.path.join(out, "_tmp")
+    os.makedirs(tmp, exist_ok=True)
+    log = open(os.path.join(out, "harness_log.jsonl"), "w")
+    meta = {"harness": "oracle/_ref/ref_harness", "modes": MODES}
+
+    # 1. pairwise distances, all modes, float and double, edge-case lengths
+    for dt, sfx in ((np.float32, "f32"), (np.float64, "f64")):
+        mix = mix_series(dt, synth.SEED_BASE + 101)
+        O.write_bundle(os.path.join(out, f"pw_mix_{sfx}.odbs"), mix)
+        for mode, (os_, oe) in MODES.items():
+            run(["pairwise", os.path.join(out, f"pw_mix_{sfx}.odbs"),
+                 os.path.join(out, f"pw_mix_{sfx}_{mode}.dist.odbs"), os_, oe], log)
+
+    # 2. plain DBA workload: 64 z-normalised random walks, lengths 512..1024, sorted
+    c1 = synth.znorm_host(synth.random_walks(64, 512, 1024, synth.SEED_BASE + 1))
+    c1 = sorted(c1, key=len)
+    O.write_bundle(os.path.join(out, "pw_c1_f32.odbs"), c1)
+    for mode in ("global", "open_end"):
+        os_, oe = MODES[mode]
+        run(["pairwise", os.path.join(out, "pw_c1_f32.odbs"),
+             os.path.join(out, f"pw_c1_f32_{mode}.dist.odbs"), os_, oe], log)
+    # approximateMedoidIndices itself: pair_dists.txt format and the medoid
+    run(["medoid", os.path.join(out, "pw_c1_f32.odbs"), os.path.join(out, "medoid_c1_f32_global"), 0, 0], log)
+
+    # 3. one DBA round, all modes, float and double (path moves as npz, two raw path files)
+    for dt, sfx in ((np.float32, "f32"), (np.float64, "f64")):
+        rng = np.random.default_rng(synth.SEED_BASE + 202)
+        lens = [200, 450, 900, 1030, 1300, 1800, 2100, 640]
+        members = []
+        for L in lens:
+            x = synth.step_signal(rng, L, 90.0, 12.0, 10.0, 2.0)
+            members.append(((x - x.mean()) / x.std()).astype(dt))
+        c = synth.step_signal(rng, 1100, 90.0, 12.0, 10.0, 2.0)
+        centroid = ((c - c.mean()) / c.std()).astype(dt)
+        O.write_bundle(os.path.join(out, f"dba_{sfx}_members.odbs"), members)
+        O.write_bundle(os.path.join(out, f"dba_{sfx}_centroid.odbs"), [centroid])
+        for mode, (os_, oe) in MODES.items():
+            pfx = os.path.join(tmp, f"dba_{sfx}_{mode}")
+            run(["dbaupdate", os.path.join(out, f"dba_{sfx}_members.odbs"),
+                 os.path.join(out, f"dba_{sfx}_centroid.odbs"), pfx, os_, oe], log)
+            for ext in (".mean.odbs", ".delta.txt"):
+                if os.path.exists(pfx + ext):
+                    shutil.copy(pfx + ext, os.path.join(out, f"dba_{sfx}_{mode}{ext}"))
+            paths_to_npz(pfx, os.path.join(out, f"dba_{sfx}_{mode}.paths.npz"))
+            if sfx == "f32" and mode in ("global", "open_end"):
+                for k in (0, 5):
+                    src = f"{pfx}.path{k}.txt"
+                    if os.path.exists(src):
+                        gz(src, os.path.join(out, f"dba_{sfx}_{mode}.path{k}.txt.gz"))
+
+    # 4. z-normalisation
+    for dt, sfx in ((np.float32, "f32"), (np.float64, "f64")):
+        rng = np.random.default_rng(synth.SEED_BASE + 303)
+        zs = [synth.step_signal(rng, L, 90.0, 12.0, 10.0, 2.0).astype(dt)
+              for L in (5, 100, 1023, 1024, 1025, 3000, 10000)]
+        O.write_bundle(os.path.join(out, f"znorm_{sfx}.odbs"), zs)
+        run(["znorm", os.path.join(out, f"znorm_{sfx}.odbs"), os.path.join(out, f"znorm_{sfx}")], log)
+
+    # 5. performDBA end to end (z-norm on), float global/open_end and double global
+    for dt, sfx, mode in ((np.float32, "f32", "global"), (np.float32, "f32", "open_end"),
+                          (np.float64, "f64", "global")):
+        rng = np.random.default_rng(synth.SEED_BASE + 404)
+        ser = [(np.cumsum(rng.standard_normal(int(L))) + 50.0).astype(dt)
+               for L in rng.integers(100, 1300, size=10)]
+        O.write_bundle(os.path.join(out, f"perform_{sfx}_{mode}.odbs"), ser)
+        pfx = os.path.join(tmp, f"perform_{sfx}_{mode}")
+        os_, oe = MODES[mode]
+        run(["performdba", os.path.join(out, f"perform_{sfx}_{mode}.odbs"), pfx, os_, oe, 1], log)
+        for ext in (".avg.txt", ".pair_dists.txt"):
+            if os.path.exists(pfx + ext):
+                shutil.copy(pfx + ext, os.path.join(out, f"perform_{sfx}_{mode}{ext}"))
+        paths_to_npz(pfx + ".0", os.path.join(out, f"perform_{sfx}_{mode}.paths.npz"))
+
+    # 6. the reference's own test sections through setupAndRun<float> (text inputs)
+    sections = {
+        "gsd": (0, 0, ["random_short1.txt", "random_short1.txt"]),
+        "gdd": (0, 0, ["random_short1.txt", "random_short2.txt"]),
+        "gtd": (0, 0, ["random_short1.txt", "random_short2.txt", "random_short3.txt"]),
+        "gdtd": (0, 1, ["random_short1.txt", "random_trun_short2.txt"]),
+        "gld": (0, 0, ["random_large0.txt", "random_large1.txt"]),
+    }
+    for name, (os_, oe, files) in sections.items():
+        pfx = os.path.join("gpurun_out", "golden_ref", "_tmp", f"sar_{name}")
+        args = ["setupandrun", pfx, os_, oe, 0] + [f"{FIXTURES}/{f}" for f in files]
+        run(args, log, cwd=ROOT)
+        for ext in (".avg.txt", ".pair_dists.txt"):
+            src = os.path.join(ROOT, pfx + ext)
+            if os.path.exists(src):
+                shutil.copy(src, os.path.join(out, f"sar_{name}{ext}"))
+
+    # 7. k-segmentation
+    for dt, sfx in ((np.float32, "f32"), (np.float64, "f64")):
+        rng = np.random.default_rng(synth.SEED_BASE + 505)
+        ss = [synth.step_signal(rng, L, 90.0, 12.0, 8.0, 1.5).astype(dt) for L in (700, 3000, 9001)]
+        O.write_bundle(os.path.join(out, f"seg_{sfx}.odbs"), ss)
+        for minseg in (4, 6):
+            run(["segment", os.path.join(out, f"seg_{sfx}.odbs"),
+                 os.path.join(out, f"seg_{sfx}_m{minseg}.odbs"), minseg, 0], log)
+
+    with open(os.path.join(out, "meta.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    shutil.rmtree(tmp, ignore_errors=True)
+
+    # 8. timing only (not a fixture): the reference's medoid launches on the first
+    # 40 rows of the 2000-series nanopore-like workload.
+    if "--timing" in sys.argv:
+        c2 = synth.znorm_host(synth.nanopore_like(2000, 2000, 8000, synth.SEED_BASE + 2))
+        c2 = sorted(c2, key=len)
+        tpath = os.path.join(ROOT, "gpurun_out", "c2_input.odbs")
+        O.write_bundle(tpath, c2)
+        p = run(["pairwise", tpath, os.path.join(ROOT, "gpurun_out", "c2_ref_rows.dist.odbs"), 0, 0, 40], log)
+        print("reference timing:", p.stdout.strip())
+        os.remove(tpath)
+    log.close()
+    print("golden written to", out)
+
+
+if __name__ == "__main__":
+    main()
