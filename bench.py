@@ -1,0 +1,351 @@
+"""Benchmark: all-vs-all DTW (the medoid pass) on one or more B200s.
+
+Workload (the metric's configuration): 2000 nanopore-like series, lengths
+uniform in [2000, 8000], piecewise-constant levels ~ N(90, 12) pA with
+geometric dwells of mean 10 samples plus N(0, 2) noise, z-normalised; global
+(unbanded) DTW of all 1,999,000 pairs in float32, then the medoid.  Seeded
+synthetic data (seed 0x0DBA0002 + rank) stands in for nanopore reads.
+
+A step is one full medoid pass: every pair's DTW distance plus the medoid
+(sums of squares, argmin).  ``value`` is whole-job DTW cell updates per second
+(GCUPS) with the z-normalised series already resident in HBM; ``e2e`` is the
+same metric through the host-buffer C entry point odba_medoid_pass_host_f32
+(pinned host series in, distances/medoid/means/sigmas out, z-normalisation on
+the device), copies inside the timed region.
+
+Multi-GPU (torchrun): every rank runs its own medoid pass on its own seeded
+data set (pairs are independent; no data-path collective), so the work per GPU
+is fixed ("weak" scaling); the step time is the max over ranks.
+
+``--impl reference`` times the reference's DTW recurrence restated in C
+(oracle/, OpenMP on all host cores, the reference itself has no CPU
+implementation) on a bounded random sample of the same workload's pairs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "all-vs-all DTW GCUPS (2000×2–8k, fp32); batched/served vs plain, p50/p99, 1 B200"
+N_SERIES, LEN_LO, LEN_HI = 2000, 2000, 8000
+SEED = 0x0DBA0002
+SMS, FP32_LANES, OPS_PER_CELL = 148, 128, 5
+SM_MAX_MHZ = 1965.0
+
+
+def workload(rank: int, n_series: int = N_SERIES):
+    from opendba_b200 import synth
+    rng = np.random.default_rng(SEED + rank)
+    lens = rng.integers(LEN_LO, LEN_HI + 1, size=n_series)
+    series = []
+    for L in lens:
+        # vectorised step signal: geometric dwells, N(90,12) levels, N(0,2) noise
+        dw = rng.geometric(0.1, size=int(L) // 4 + 16)
+        while dw.sum() < L:
+            dw = np.concatenate([dw, rng.geometric(0.1, size=int(L) // 4 + 16)])
+        levels = rng.normal(90.0, 12.0, size=len(dw))
+        x = np.repeat(levels, dw)[:L] + rng.normal(0.0, 2.0, size=int(L))
+        series.append(x.astype(np.float32))
+    series.sort(key=len)  # performDBA sorts by length before the medoid pass (dba.hpp:876-885)
+    return series, synth
+
+
+def cells_of(lens) -> float:
+    lens = np.asarray(lens, dtype=np.float64)
+    tot = lens.sum()
+    return float((tot * tot - (lens * lens).sum()) / 2.0)
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.out.flush()
+
+    def summary(self):
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        clocks, reasons, maxc = [], set(), SM_MAX_MHZ
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                clocks.append(float(r[1]))
+                maxc = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not clocks:
+            return {"sm_mhz": None, "sm_max_mhz": SM_MAX_MHZ, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(clocks), "sm_max_mhz": maxc, "reasons": sorted(reasons),
+                "samples": len(clocks)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(series, target_secs: float, seed: int = 7):
+    """Times the C restatement (OpenMP, all host threads) on a random pair sample."""
+    from oracle import oracle as O
+    O.lib()
+    n = len(series)
+    npairs = n * (n - 1) // 2
+    lens = np.array([len(s) for s in series], dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(n - 1), np.arange(n - 1, 0, -1))
+    starts = np.concatenate([[0], np.cumsum(np.arange(n - 1, 0, -1))])[:-1]
+    cols = np.arange(npairs) - np.repeat(starts, np.arange(n - 1, 0, -1)) + rows + 1
+    threads = os.cpu_count() or 1
+    # calibrate on a small sample, then size the measured sample to ~target_secs
+    probe = rng.choice(npairs, size=max(threads, 8), replace=False)
+    t0 = time.perf_counter()
+    O.pairwise_fast(series, 0, 0, pair_list=probe, threads=threads)
+    dt = time.perf_counter() - t0
+    rate = float((lens[rows[probe]] * lens[cols[probe]]).sum()) / max(dt, 1e-6)
+    per_pair = float((lens[rows] * lens[cols]).mean())
+    k = int(max(threads, min(npairs, target_secs * rate / per_pair)))
+    sample = rng.choice(npairs, size=k, replace=False)
+    cells = float((lens[rows[sample]] * lens[cols[sample]]).sum())
+    t0 = time.perf_counter()
+    O.pairwise_fast(series, 0, 0, pair_list=sample, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+            "sample": f"{k} random pairs of the same workload ({cells:.3e} cells, {dt:.1f} s), "
+                      "distance-only C restatement of dtw.hpp:158-239, OpenMP over pairs"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    series, _ = workload(0)
+    series = [s for s in series]
+    from opendba_b200 import synth
+    series = synth.znorm_host(series)
+    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_baseline(series, per_step * 0.3, seed=11)
+    vals, secs = [], []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        cb = cpu_baseline(series, per_step, seed=100 + i)
+        secs.append(time.perf_counter() - t0)
+        vals.append(cb["value"])
+    v = float(statistics.mean(vals))
+    cb["value"] = v
+    line = {
+        "metric": METRIC, "value": v, "unit": "GCUPS", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(secs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded nanopore-like step signals)",
+        "config": {"workload": f"medoid all-vs-all: {N_SERIES} series, lengths U[{LEN_LO},{LEN_HI}], "
+                               "global DTW, float32, z-normalised",
+                   "series": N_SERIES, "len_range": [LEN_LO, LEN_HI], "mode": "global",
+                   "sample": "random pairs per step (CPU)"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "GCUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-secs", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--n-series", type=int, default=N_SERIES,
+                    help="development only: fewer series than the benchmark configuration")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=device)
+    from opendba_b200 import api, build, _native
+    if not os.path.exists(_native.LIB_PATH):
+        build.build_library()
+    series_raw, synth = workload(rank, args.n_series)
+    lens = [len(s) for s in series_raw]
+    cells = cells_of(lens)
+    stream = torch.cuda.current_stream()
+
+    # resident, z-normalised inputs for the device-side value
+    ds = api.DeviceSeries.from_host(series_raw)
+    api.znorm_(ds)
+    ws = api.pairwise_workspace(ds)
+    out = torch.empty(len(lens) * (len(lens) - 1) // 2, dtype=torch.float32, device=device)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MiB > L2
+
+    def step(evk=None):
+        if evk is not None:
+            evk[0].record(stream)
+        api.pairwise(ds, 0, 0, out=out, workspace=ws, stream=stream)
+        if evk is not None:
+            evk[1].record(stream)
+        return api.medoid(out, ds, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    step_ms, kern_ms = [], []
+    medoid_idx = None
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(float(i))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            _, medoid_idx = step((k0, k1))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            kern_ms.append(k0.elapsed_time(k1))
+    clocks = clk.summary()
+    barrier(world)
+    ms = max_over_ranks(statistics.mean(step_ms), world, device)
+    kms = max_over_ranks(statistics.mean(kern_ms), world, device)
+    value = world * cells / (ms * 1e-3) / 1e9
+
+    # end to end through the host-buffer C entry point (pinned host input)
+    flat, _, hl = api.pack_host(series_raw)
+    pinned = torch.from_numpy(flat).pin_memory()
+    flat_p = pinned.numpy()
+    npairs = len(lens) * (len(lens) - 1) // 2
+    dists_h = torch.empty(npairs, dtype=torch.float32).pin_memory().numpy()
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
+    api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)  # warm-up
+    barrier(world)
+    e2e_s = []
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, med_e2e, _, _ = api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_sec = max_over_ranks(statistics.mean(e2e_s), world, device)
+    e2e_value = world * cells / e2e_sec / 1e9
+    h2d = flat.nbytes + 2 * 8 * len(lens)
+    d2h = npairs * 4 + 4 + 2 * 8 * len(lens)
+
+    f_mhz = clocks["sm_mhz"] or SM_MAX_MHZ
+    peak = SMS * FP32_LANES * f_mhz * 1e6 / OPS_PER_CELL / 1e9
+    peak_max = SMS * FP32_LANES * SM_MAX_MHZ * 1e6 / OPS_PER_CELL / 1e9
+    achieved = cells / (kms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "pairwise_dtw_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    hbm_gbs = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hbm_gbs = json.load(f).get("hbm_gbs")
+    except OSError:
+        pass
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded nanopore-like step signals)",
+            "config": {"workload": f"medoid all-vs-all: {args.n_series} series, lengths U[{LEN_LO},{LEN_HI}], "
+                                   "global DTW, float32, z-normalised",
+                       "series": args.n_series, "pairs": npairs, "cells_per_gpu": cells,
+                       "len_range": [LEN_LO, LEN_HI], "mode": "global", "parallelism": f"pairs dp{world}",
+                       "l2": "256 MiB buffer written between timed steps"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "GCUPS",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_basis": f"{SMS} SMs x {FP32_LANES} FP32 lanes x {f_mhz:.0f} MHz "
+                                       f"(median sampled) / {OPS_PER_CELL} ops per cell",
+                         "frac_at_max_clock": achieved / peak_max,
+                         "kernel": "pairwise_kernel<float,32,4>", "kernel_ms": kms,
+                         "hbm_peak_gbs_measured": hbm_gbs},
+            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_sec,
+                    "api": "odba_medoid_pass_host_f32 (z-norm + pairwise + medoid, pinned host buffers)"},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+            "medoid": medoid_idx, "medoid_e2e": med_e2e,
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline(synth.znorm_host(series_raw), args.cpu_secs)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

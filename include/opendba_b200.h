@@ -1,0 +1,98 @@
+/* opendba_b200 -- C ABI of the B200 (sm_100a) implementation of OpenDBA's
+ * data-parallel hot path: the all-vs-all DTW medoid pass, z-normalisation and
+ * the DBA round (DTW with warp path, backtrack, centroid update).
+ *
+ * The reference (Brooklynvcx/OpenDBA) has no library or FFI: its API is the
+ * header-only C++ templates in dba.hpp / gpu_utils.hpp included into one
+ * translation unit.  Each entry point below replaces one of those, as cited.
+ * All functions return an odba_status; on failure odba_last_error() gives a
+ * message (per calling thread).  Device pointers are plain CUDA device (or
+ * managed) addresses; "stream" is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  No function keeps a pointer after it returns.
+ *
+ * Series layout on the device: the n series are concatenated in one array;
+ * series i starts at element offsets[i] and has lens[i] elements (>= 1).
+ * Pair distances use the reference's upper-triangle order: pair (s, j), s < j,
+ * at index s*n - s*(s+1)/2 + (j - s - 1) (clustering.cuh:4-6).
+ */
+#ifndef OPENDBA_B200_H
+#define OPENDBA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ODBA_ABI_VERSION 1
+
+enum odba_status {
+  ODBA_OK = 0,
+  ODBA_ERR_INVALID_ARGUMENT = 1,
+  ODBA_ERR_CUDA = 2,
+  ODBA_ERR_OUT_OF_MEMORY = 3,
+  ODBA_ERR_WORKSPACE_TOO_SMALL = 4,
+  ODBA_ERR_UNSUPPORTED_DEVICE = 5,
+  ODBA_ERR_TIMEOUT = 6,
+  ODBA_ERR_IO = 7
+};
+
+int odba_abi_version(void);
+const char *odba_status_string(int status);
+/* Message of the last failure in the calling thread ("" if none). */
+const char *odba_last_error(void);
+/* ODBA_OK when the current CUDA device is a compute capability 10.x (B200) part. */
+int odba_device_check(void);
+
+/* ---- all-vs-all DTW distances (the medoid pass) ----------------------------
+ * Replaces the DTWDistance launch loop of approximateMedoidIndices
+ * (dba.hpp:37-161, kernel dtw.hpp:39-259) for one device.  Series s is the
+ * first (row) series of pair (s, j), as in the reference.  The workspace holds
+ * a work counter and per-warp swath-edge buffers; its size depends only on the
+ * element size and the longest series.  use_open_start / use_open_end have the
+ * reference's meaning (openDBA.cu:72-104). */
+size_t odba_dtw_pairwise_workspace_bytes(int elem_size, uint64_t max_len);
+int odba_dtw_pairwise_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                          int n, uint64_t max_len, int use_open_start, int use_open_end,
+                          float *dists, void *workspace, size_t workspace_bytes, void *stream);
+int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                          int n, uint64_t max_len, int use_open_start, int use_open_end,
+                          double *dists, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- medoid from pair distances (one cluster) ------------------------------
+ * Replaces the sum-of-squares and medoid choice of approximateMedoidIndices
+ * (dba.hpp:186-203, 325-342).  sos (n values) and medoid (one int) are device
+ * buffers; lens are the device series lengths (used when n == 2). */
+int odba_medoid_f32(const float *dists, const uint64_t *lens, int n, float *sos, int *medoid,
+                    void *stream);
+int odba_medoid_f64(const double *dists, const uint64_t *lens, int n, double *sos, int *medoid,
+                    void *stream);
+
+/* ---- z-normalisation in place ----------------------------------------------
+ * Replaces normalizeSequences<T> with refSequenceIndex < 0 (gpu_utils.hpp:132-170).
+ * means / sigmas (n doubles, device) may be NULL. */
+int odba_znorm_f32(float *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                   double *means, double *sigmas, void *stream);
+int odba_znorm_f64(double *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                   double *means, double *sigmas, void *stream);
+
+/* ---- host-buffer medoid pass (end to end) ------------------------------------
+ * What performDBA does between its sort and the DBA rounds for one cluster
+ * (dba.hpp:902-928 with approximateMedoidIndices): copies the concatenated
+ * host series to the device, optionally z-normalises them, computes all pair
+ * distances and the medoid, and copies the distances (n(n-1)/2), the medoid
+ * index and, when norm != 0, the per-series means and sigmas back.  Host
+ * buffers may be pageable or pinned; h_means / h_sigmas may be NULL. */
+int odba_medoid_pass_host_f32(const float *h_series, const uint64_t *h_lens, int n,
+                              int use_open_start, int use_open_end, int norm, float *h_dists,
+                              int *h_medoid, double *h_means, double *h_sigmas, void *stream);
+int odba_medoid_pass_host_f64(const double *h_series, const uint64_t *h_lens, int n,
+                              int use_open_start, int use_open_end, int norm, double *h_dists,
+                              int *h_medoid, double *h_means, double *h_sigmas, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPENDBA_B200_H */

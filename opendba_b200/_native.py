@@ -1,0 +1,73 @@
+"""ctypes binding of libopendba_b200.so (the C ABI in include/opendba_b200.h).
+
+The library is built in-tree by ``opendba_b200.build.build_library()``.  There
+is no fallback: if the shared library is missing or fails to load, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libopendba_b200.so")
+
+ODBA_OK = 0
+STATUS_NAMES = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
+    4: "workspace too small", 5: "unsupported device", 6: "timed out", 7: "I/O error",
+}
+
+_lib = None
+
+P = ctypes.c_void_p
+U64 = ctypes.c_uint64
+I32 = ctypes.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "odba_abi_version": (I32, []),
+    "odba_status_string": (ctypes.c_char_p, [I32]),
+    "odba_last_error": (ctypes.c_char_p, []),
+    "odba_device_check": (I32, []),
+    "odba_dtw_pairwise_workspace_bytes": (ctypes.c_size_t, [I32, U64]),
+    "odba_dtw_pairwise_f32": (I32, [P, P, P, I32, U64, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_dtw_pairwise_f64": (I32, [P, P, P, I32, U64, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_medoid_f32": (I32, [P, P, I32, P, P, P]),
+    "odba_medoid_f64": (I32, [P, P, I32, P, P, P]),
+    "odba_znorm_f32": (I32, [P, P, P, I32, P, P, P]),
+    "odba_znorm_f64": (I32, [P, P, P, I32, P, P, P]),
+    "odba_medoid_pass_host_f32": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
+    "odba_medoid_pass_host_f64": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
+}
+
+
+class OdbaError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the native library (once).  Raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OdbaError(2, f"native library not built: {LIB_PATH} (run opendba_b200.build)")
+        _lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(_lib, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != ODBA_OK:
+        raise OdbaError(status, lib().odba_last_error().decode(errors="replace"))
+
+
+def call(name: str, *args) -> int:
+    """Calls an entry point that returns an odba_status and raises on failure."""
+    check(getattr(lib(), name)(*args))
+    return 0

@@ -1,0 +1,144 @@
+"""Python host API over the C ABI.
+
+Mirrors the reference's entry points for the hot path (names and argument
+meaning of dba.hpp / gpu_utils.hpp): all-vs-all DTW distances and the medoid
+(approximateMedoidIndices, dba.hpp:37), z-normalisation (normalizeSequences,
+gpu_utils.hpp:133).  Device memory comes from PyTorch tensors; PyTorch is only
+the allocator and stream provider here, every computation runs in
+libopendba_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+
+_SFX = {np.dtype(np.float32): "f32", np.dtype(np.float64): "f64"}
+
+
+def _torch():
+    import torch  # noqa: WPS433 (deferred: only device-side helpers need it)
+    return torch
+
+
+def _stream_ptr(stream) -> int | None:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def pack_host(series, dtype=None):
+    """Concatenates a ragged list of 1-D arrays: (flat, offsets, lens) numpy arrays."""
+    dtype = np.dtype(dtype or np.asarray(series[0]).dtype)
+    if dtype not in _SFX:
+        raise TypeError("series must be float32 or float64")
+    lens = np.array([len(s) for s in series], dtype=np.uint64)
+    if np.any(lens == 0):
+        raise ValueError("every series needs at least one sample")
+    offsets = np.zeros(len(series), dtype=np.uint64)
+    if len(series) > 1:
+        offsets[1:] = np.cumsum(lens)[:-1]
+    flat = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=dtype) for s in series]))
+    return flat, offsets, lens
+
+
+@dataclass
+class DeviceSeries:
+    """A ragged set of series resident in device memory (concatenated)."""
+    data: "object"      # torch tensor, float32/float64, on cuda
+    offsets: "object"   # torch uint64 tensor (device)
+    lens: "object"      # torch uint64 tensor (device)
+    host_lens: np.ndarray
+    dtype: np.dtype
+
+    @property
+    def n(self) -> int:
+        return len(self.host_lens)
+
+    @property
+    def max_len(self) -> int:
+        return int(self.host_lens.max()) if self.n else 0
+
+    @classmethod
+    def from_host(cls, series, dtype=None, device="cuda") -> "DeviceSeries":
+        torch = _torch()
+        flat, offsets, lens = pack_host(series, dtype)
+        # pad the tail so vector loads past the last sample stay inside the allocation
+        padded = np.concatenate([flat, np.zeros(16, dtype=flat.dtype)])
+        data = torch.from_numpy(padded).to(device)
+        off = torch.from_numpy(offsets.view(np.int64)).to(device)
+        ln = torch.from_numpy(lens.view(np.int64)).to(device)
+        return cls(data, off, ln, lens, flat.dtype)
+
+    def to_host(self) -> list[np.ndarray]:
+        flat = self.data.cpu().numpy()
+        offs = self.offsets.cpu().numpy().view(np.uint64)
+        return [flat[int(o):int(o) + int(L)].copy() for o, L in zip(offs, self.host_lens)]
+
+
+def pairwise_workspace(ds: DeviceSeries):
+    torch = _torch()
+    nbytes = _native.lib().odba_dtw_pairwise_workspace_bytes(ds.dtype.itemsize, ds.max_len)
+    return torch.empty(nbytes, dtype=torch.uint8, device=ds.data.device)
+
+
+def pairwise(ds: DeviceSeries, open_start: int = 0, open_end: int = 0, out=None, workspace=None,
+             stream=None):
+    """All pair distances (upper triangle, reference order) as a device tensor."""
+    torch = _torch()
+    n = ds.n
+    npairs = n * (n - 1) // 2
+    if out is None:
+        out = torch.empty(max(npairs, 1), dtype=ds.data.dtype, device=ds.data.device)
+    if workspace is None:
+        workspace = pairwise_workspace(ds)
+    _native.call(f"odba_dtw_pairwise_{_SFX[ds.dtype]}", ds.data.data_ptr(), ds.offsets.data_ptr(),
+                 ds.lens.data_ptr(), n, ds.max_len, int(open_start), int(open_end), out.data_ptr(),
+                 workspace.data_ptr(), workspace.numel(), _stream_ptr(stream))
+    return out[:npairs]
+
+
+def medoid(dists, ds: DeviceSeries, stream=None):
+    """(sums of squares tensor, medoid index) for one cluster of ds."""
+    torch = _torch()
+    sos = torch.empty(ds.n, dtype=ds.data.dtype, device=ds.data.device)
+    med = torch.empty(1, dtype=torch.int32, device=ds.data.device)
+    _native.call(f"odba_medoid_{_SFX[ds.dtype]}", dists.data_ptr() if dists.numel() else None,
+                 ds.lens.data_ptr(), ds.n, sos.data_ptr(), med.data_ptr(), _stream_ptr(stream))
+    return sos, int(med.item())
+
+
+def znorm_(ds: DeviceSeries, stream=None):
+    """Z-normalises ds in place; returns (means, sigmas) device tensors (float64)."""
+    torch = _torch()
+    means = torch.empty(ds.n, dtype=torch.float64, device=ds.data.device)
+    sigmas = torch.empty(ds.n, dtype=torch.float64, device=ds.data.device)
+    _native.call(f"odba_znorm_{_SFX[ds.dtype]}", ds.data.data_ptr(), ds.offsets.data_ptr(),
+                 ds.lens.data_ptr(), ds.n, means.data_ptr(), sigmas.data_ptr(), _stream_ptr(stream))
+    return means, sigmas
+
+
+def medoid_pass_host(series, open_start: int = 0, open_end: int = 0, norm: int = 1,
+                     dtype=None, flat=None, lens=None, dists_out=None, stream=None):
+    """End-to-end medoid pass through the host-buffer C entry point.
+
+    Either a list of series, or pre-packed ``flat``/``lens`` host arrays (pinned
+    or pageable) may be given.  Returns (dists, medoid, means, sigmas)."""
+    if flat is None:
+        flat, _, lens = pack_host(series, dtype)
+    dt = np.dtype(flat.dtype)
+    n = len(lens)
+    npairs = n * (n - 1) // 2
+    if dists_out is None:
+        dists_out = np.empty(max(npairs, 1), dtype=dt)
+    med = np.zeros(1, dtype=np.int32)
+    means = np.zeros(n, dtype=np.float64)
+    sigmas = np.zeros(n, dtype=np.float64)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _native.call(f"odba_medoid_pass_host_{_SFX[dt]}", vp(flat), vp(np.ascontiguousarray(lens, dtype=np.uint64)),
+                 n, int(open_start), int(open_end), int(norm), vp(dists_out), vp(med),
+                 vp(means), vp(sigmas), stream)
+    return dists_out[:npairs], int(med[0]), means, sigmas

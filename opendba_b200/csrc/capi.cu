@@ -1,0 +1,229 @@
+// The extern "C" surface of libopendba_b200.so (include/opendba_b200.h):
+// argument validation, error reporting and the host-buffer entry points.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "odba_internal.h"
+
+namespace odba {
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+int fail(int status, const char *msg) {
+  std::snprintf(g_err, sizeof(g_err), "%s", msg);
+  return status;
+}
+
+int check_launch(const char *what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return ODBA_OK;
+  char buf[400];
+  std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  return fail(e == cudaErrorMemoryAllocation ? ODBA_ERR_OUT_OF_MEMORY : ODBA_ERR_CUDA, buf);
+}
+
+int require_sm100() {
+  int dev = 0, major = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess)
+    return fail(ODBA_ERR_CUDA, "no CUDA device available");
+  if (major != 10) return fail(ODBA_ERR_UNSUPPORTED_DEVICE, "requires a compute capability 10.x (sm_100a) device");
+  return ODBA_OK;
+}
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  char buf[400];
+  std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+  return fail(e == cudaErrorMemoryAllocation ? ODBA_ERR_OUT_OF_MEMORY : ODBA_ERR_CUDA, buf);
+}
+
+#define ODBA_CUDA(call, what)                       \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+template <typename T>
+int pairwise_checked(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                     uint64_t max_len, int os, int oe, T *dists, void *ws, size_t ws_bytes,
+                     void *stream) {
+  if (n < 0 || (n >= 2 && (!series || !offsets || !lens || !dists || !ws)))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or negative series count");
+  if (max_len == 0 || max_len > (1ull << 31))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be in [1, 2^31]");
+  if (int rc = require_sm100()) return rc;
+  return pairwise_launch<T>(series, offsets, lens, n, max_len, os ? 1 : 0, oe ? 1 : 0, dists, ws,
+                            ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
+template <typename T>
+int medoid_pass_host(const T *h_series, const uint64_t *h_lens, int n, int os, int oe, int norm,
+                     T *h_dists, int *h_medoid, double *h_means, double *h_sigmas, void *stream_v) {
+  if (n < 1 || !h_series || !h_lens || !h_medoid || (n >= 2 && !h_dists))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or empty input");
+  if (int rc = require_sm100()) return rc;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_v);
+  std::vector<uint64_t> offs(n);
+  uint64_t total = 0, max_len = 0;
+  for (int i = 0; i < n; ++i) {
+    if (h_lens[i] == 0) return fail(ODBA_ERR_INVALID_ARGUMENT, "every series needs at least one sample");
+    offs[i] = total;
+    total += h_lens[i];
+    if (h_lens[i] > max_len) max_len = h_lens[i];
+  }
+  const size_t npairs = size_t(n) * (n - 1) / 2;
+  const size_t ws_bytes = pairwise_workspace_bytes<T>(max_len);
+  // one device allocation: series | offsets | lens | dists | sos | means | sigmas | medoid | workspace
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_series = up((total + 16) * sizeof(T)), b_meta = up(n * sizeof(uint64_t)),
+               b_d = up((npairs + 1) * sizeof(T)), b_sos = up(n * sizeof(T)),
+               b_mv = up(n * sizeof(double)), b_med = 256;
+  const size_t bytes = b_series + 2 * b_meta + b_d + b_sos + 2 * b_mv + b_med + ws_bytes;
+  char *base = nullptr;
+  ODBA_CUDA(cudaMallocAsync(reinterpret_cast<void **>(&base), bytes, stream), "device allocation");
+  T *d_series = reinterpret_cast<T *>(base);
+  uint64_t *d_offs = reinterpret_cast<uint64_t *>(base + b_series);
+  uint64_t *d_lens = reinterpret_cast<uint64_t *>(base + b_series + b_meta);
+  T *d_dists = reinterpret_cast<T *>(base + b_series + 2 * b_meta);
+  T *d_sos = reinterpret_cast<T *>(base + b_series + 2 * b_meta + b_d);
+  double *d_means = reinterpret_cast<double *>(base + b_series + 2 * b_meta + b_d + b_sos);
+  double *d_sigmas = d_means + b_mv / sizeof(double);
+  int *d_medoid = reinterpret_cast<int *>(base + b_series + 2 * b_meta + b_d + b_sos + 2 * b_mv);
+  void *d_ws = base + b_series + 2 * b_meta + b_d + b_sos + 2 * b_mv + b_med;
+  int rc = ODBA_OK;
+  auto run = [&]() -> int {
+    ODBA_CUDA(cudaMemcpyAsync(d_series, h_series, total * sizeof(T), cudaMemcpyHostToDevice, stream),
+              "series upload");
+    ODBA_CUDA(cudaMemcpyAsync(d_offs, offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, stream),
+              "offsets upload");
+    ODBA_CUDA(cudaMemcpyAsync(d_lens, h_lens, n * sizeof(uint64_t), cudaMemcpyHostToDevice, stream),
+              "lengths upload");
+    if (norm) {
+      if (int r = znorm_launch<T>(d_series, d_offs, d_lens, n, d_means, d_sigmas, stream)) return r;
+    }
+    if (n >= 2) {
+      if (int r = pairwise_launch<T>(d_series, d_offs, d_lens, n, max_len, os ? 1 : 0, oe ? 1 : 0,
+                                     d_dists, d_ws, ws_bytes, stream))
+        return r;
+    }
+    if (int r = medoid_launch<T>(d_dists, d_lens, n, d_sos, d_medoid, stream)) return r;
+    if (n >= 2)
+      ODBA_CUDA(cudaMemcpyAsync(h_dists, d_dists, npairs * sizeof(T), cudaMemcpyDeviceToHost, stream),
+                "distance download");
+    ODBA_CUDA(cudaMemcpyAsync(h_medoid, d_medoid, sizeof(int), cudaMemcpyDeviceToHost, stream),
+              "medoid download");
+    if (norm && h_means)
+      ODBA_CUDA(cudaMemcpyAsync(h_means, d_means, n * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                "means download");
+    if (norm && h_sigmas)
+      ODBA_CUDA(cudaMemcpyAsync(h_sigmas, d_sigmas, n * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                "sigmas download");
+    ODBA_CUDA(cudaStreamSynchronize(stream), "medoid pass");
+    return ODBA_OK;
+  };
+  rc = run();
+  cudaFreeAsync(base, stream);
+  if (rc == ODBA_OK) ODBA_CUDA(cudaStreamSynchronize(stream), "medoid pass teardown");
+  return rc;
+}
+
+}  // namespace
+}  // namespace odba
+
+using namespace odba;
+
+extern "C" {
+
+int odba_abi_version(void) { return ODBA_ABI_VERSION; }
+
+const char *odba_status_string(int status) {
+  switch (status) {
+    case ODBA_OK: return "ok";
+    case ODBA_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case ODBA_ERR_CUDA: return "CUDA error";
+    case ODBA_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case ODBA_ERR_WORKSPACE_TOO_SMALL: return "workspace too small";
+    case ODBA_ERR_UNSUPPORTED_DEVICE: return "unsupported device";
+    case ODBA_ERR_TIMEOUT: return "timed out";
+    case ODBA_ERR_IO: return "I/O error";
+    default: return "unknown status";
+  }
+}
+
+const char *odba_last_error(void) { return odba::g_err; }
+
+int odba_device_check(void) { return require_sm100(); }
+
+size_t odba_dtw_pairwise_workspace_bytes(int elem_size, uint64_t max_len) {
+  if (elem_size == 8) return pairwise_workspace_bytes<double>(max_len);
+  return pairwise_workspace_bytes<float>(max_len);
+}
+
+int odba_dtw_pairwise_f32(const float *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                          uint64_t max_len, int use_open_start, int use_open_end, float *dists,
+                          void *workspace, size_t workspace_bytes, void *stream) {
+  return pairwise_checked<float>(series, offsets, lens, n, max_len, use_open_start, use_open_end,
+                                 dists, workspace, workspace_bytes, stream);
+}
+
+int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                          int n, uint64_t max_len, int use_open_start, int use_open_end,
+                          double *dists, void *workspace, size_t workspace_bytes, void *stream) {
+  return pairwise_checked<double>(series, offsets, lens, n, max_len, use_open_start, use_open_end,
+                                  dists, workspace, workspace_bytes, stream);
+}
+
+int odba_medoid_f32(const float *dists, const uint64_t *lens, int n, float *sos, int *medoid,
+                    void *stream) {
+  if (n < 1 || !lens || !sos || !medoid || (n >= 2 && !dists))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or empty input");
+  if (int rc = require_sm100()) return rc;
+  return medoid_launch<float>(dists, lens, n, sos, medoid, static_cast<cudaStream_t>(stream));
+}
+
+int odba_medoid_f64(const double *dists, const uint64_t *lens, int n, double *sos, int *medoid,
+                    void *stream) {
+  if (n < 1 || !lens || !sos || !medoid || (n >= 2 && !dists))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or empty input");
+  if (int rc = require_sm100()) return rc;
+  return medoid_launch<double>(dists, lens, n, sos, medoid, static_cast<cudaStream_t>(stream));
+}
+
+int odba_znorm_f32(float *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                   double *means, double *sigmas, void *stream) {
+  if (n < 0 || (n > 0 && (!series || !offsets || !lens)))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or negative series count");
+  if (int rc = require_sm100()) return rc;
+  return znorm_launch<float>(series, offsets, lens, n, means, sigmas, static_cast<cudaStream_t>(stream));
+}
+
+int odba_znorm_f64(double *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                   double *means, double *sigmas, void *stream) {
+  if (n < 0 || (n > 0 && (!series || !offsets || !lens)))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or negative series count");
+  if (int rc = require_sm100()) return rc;
+  return znorm_launch<double>(series, offsets, lens, n, means, sigmas, static_cast<cudaStream_t>(stream));
+}
+
+int odba_medoid_pass_host_f32(const float *h_series, const uint64_t *h_lens, int n,
+                              int use_open_start, int use_open_end, int norm, float *h_dists,
+                              int *h_medoid, double *h_means, double *h_sigmas, void *stream) {
+  return medoid_pass_host<float>(h_series, h_lens, n, use_open_start, use_open_end, norm, h_dists,
+                                 h_medoid, h_means, h_sigmas, stream);
+}
+
+int odba_medoid_pass_host_f64(const double *h_series, const uint64_t *h_lens, int n,
+                              int use_open_start, int use_open_end, int norm, double *h_dists,
+                              int *h_medoid, double *h_means, double *h_sigmas, void *stream) {
+  return medoid_pass_host<double>(h_series, h_lens, n, use_open_start, use_open_end, norm, h_dists,
+                                  h_medoid, h_means, h_sigmas, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,219 @@
+// All-vs-all DTW distances for the medoid pass: the work of
+// approximateMedoidIndices' launch loop (dba.hpp:67-161) and the pair-distance
+// epilogue of DTWDistance (dtw.hpp:116-125, 242-257), as one persistent launch.
+//
+// Every warp of the grid pulls pairs from a device work counter, largest pair
+// index first (with length-sorted input that is roughly largest cost first),
+// and sweeps the pair swath by swath with the register wavefront of
+// dtw_device.cuh.  The swath right-edge column goes through a per-warp
+// ping-pong buffer in global memory (L2-resident in practice).
+//
+// Output: the reference's upper-triangle layout, pair (s, j), s < j, at
+// index s*n - s*(s+1)/2 + (j - s - 1) (clustering.cuh:4-6), with
+//   dist = (T) sqrtf(C[m-1][n-1])           global / open modes
+//   dist = (T)(sqrtf(C[m-1][n-1]) / m)      exactly one open end
+// computed in float like the reference (sqrtf even for double, dtw.hpp:121,251,254).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "dtw_device.cuh"
+#include "odba_internal.h"
+
+namespace odba {
+
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+
+template <typename T>
+struct PairwiseArgs {
+  const T *series;
+  const uint64_t *offsets;
+  const uint64_t *lens;
+  int n;
+  unsigned long long npairs;
+  T *dists;
+  unsigned long long *counter;
+  T *edges;
+  unsigned long long edge_stride;  // elements per edge buffer
+  int open_start, open_end;
+};
+
+__device__ __forceinline__ long long row_start(long long s, long long n) {
+  return s * n - s * (s + 1) / 2;
+}
+
+// Upper-triangle pair index -> (s, j).
+__device__ __forceinline__ void pair_of(long long p, long long n, int &s_out, int &j_out) {
+  const double b = 2.0 * double(n) - 1.0;
+  long long s = (long long)((b - sqrt(b * b - 8.0 * double(p))) * 0.5);
+  if (s < 0) s = 0;
+  if (s > n - 2) s = n - 2;
+  while (s + 1 <= n - 2 && row_start(s + 1, n) <= p) ++s;
+  while (s > 0 && row_start(s, n) > p) --s;
+  s_out = int(s);
+  j_out = int(s + 1 + (p - row_start(s, n)));
+}
+
+template <typename T>
+__device__ __forceinline__ T pair_distance(T corner, int m, int n, int os, int oe) {
+  float v;
+  if (m == 1 && oe && !os && n > kRefSwath) {
+    // single-row matrix: the reference's open-end shortcut reads back the
+    // sentinel it has just stored (dtw.hpp:113, 121)
+    v = __fdiv_rn(__fsqrt_rn(float(Num<T>::big())), float(m));
+  } else if ((oe && !os) || (!oe && os)) {
+    v = __fdiv_rn(__fsqrt_rn(float(corner)), float(m));
+  } else {
+    v = __fsqrt_rn(float(corner));
+  }
+  return T(v);
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void run_swath(const SwathJob<T> &job, bool last, T &corner) {
+  T col[R];
+  sweep_swath<T, R>(job, col);
+  if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
+}
+
+// Full swaths use RF registers per lane (swath width 32*RF); the last, partial
+// swath uses the smallest multiple of RQ registers that covers it.
+template <typename T, int RF, int RQ>
+__device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
+  constexpr int W = 32 * RF;
+  int k = 0;
+  for (int c0 = 0; c0 < job.n; c0 += W, ++k) {
+    const int width = job.n - c0 < W ? job.n - c0 : W;
+    const bool last = c0 + W >= job.n;
+    job.c0 = c0;
+    // ping-pong: swath k writes buffer k%2 and reads buffer (k+1)%2
+    job.edge_in = c0 ? ((k & 1) ? e0 : e1) : nullptr;
+    job.edge_out = last ? nullptr : ((k & 1) ? e1 : e0);
+    job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
+    job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
+    const int rneed = (width + 31) / 32;
+    const int rq = (rneed + RQ - 1) / RQ * RQ;
+    if (rq >= RF) {
+      run_swath<T, RF>(job, last, corner);
+    } else {
+      switch (rq / RQ) {
+#define ODBA_CASE(K)                                          \
+  case K:                                                     \
+    if constexpr (K * RQ < RF) run_swath<T, K * RQ>(job, last, corner); \
+    break;
+        ODBA_CASE(1)
+        ODBA_CASE(2)
+        ODBA_CASE(3)
+        ODBA_CASE(4)
+        ODBA_CASE(5)
+        ODBA_CASE(6)
+        ODBA_CASE(7)
+#undef ODBA_CASE
+        default:
+          break;
+      }
+    }
+    // the next swath's lane 0 reads what this swath's lane 31 wrote
+    __syncwarp();
+  }
+}
+
+template <typename T, int RF, int RQ>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    pairwise_kernel(PairwiseArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  T *e0 = a.edges + slot * 2 * a.edge_stride;
+  T *e1 = e0 + a.edge_stride;
+  for (;;) {
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(a.counter, 1ull);
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= a.npairs) break;
+    const long long p = (long long)(a.npairs - 1 - q);
+    int s, j;
+    pair_of(p, a.n, s, j);
+    SwathJob<T> job;
+    job.x = a.series + a.offsets[s];
+    job.m = int(a.lens[s]);
+    job.y = a.series + a.offsets[j];
+    job.n = int(a.lens[j]);
+    job.r0 = a.open_start ? 1 : 0;
+    job.open_end = a.open_end != 0;
+    T corner = T(0);
+    sweep_pair<T, RF, RQ>(job, e0, e1, corner);
+    if (lane == 0) a.dists[p] = pair_distance<T>(corner, job.m, job.n, a.open_start, a.open_end);
+  }
+}
+
+template <typename T>
+struct Tune;
+template <>
+struct Tune<float> {
+  static constexpr int RF = 32, RQ = 4;
+};
+template <>
+struct Tune<double> {
+  static constexpr int RF = 16, RQ = 4;
+};
+
+template <typename T>
+int grid_size() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && cached[dev]) return cached[dev];
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ>, kWarpsPerBlock * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int g = sms * per_sm;
+  if (dev < 64) cached[dev] = g;
+  return g;
+}
+
+}  // namespace
+
+template <typename T>
+size_t pairwise_workspace_bytes(uint64_t max_len) {
+  const unsigned long long stride = (max_len + 32 + 31) / 32 * 32;
+  const size_t slots = size_t(grid_size<T>()) * kWarpsPerBlock;
+  return 256 + slots * 2 * stride * sizeof(T);
+}
+
+template <typename T>
+int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                    uint64_t max_len, int os, int oe, T *dists, void *workspace, size_t ws_bytes,
+                    cudaStream_t stream) {
+  if (n < 2) return ODBA_OK;
+  const size_t need = pairwise_workspace_bytes<T>(max_len);
+  if (ws_bytes < need) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "workspace too small");
+  PairwiseArgs<T> a;
+  a.series = series;
+  a.offsets = offsets;
+  a.lens = lens;
+  a.n = n;
+  a.npairs = (unsigned long long)n * (n - 1) / 2;
+  a.dists = dists;
+  a.counter = static_cast<unsigned long long *>(workspace);
+  a.edges = reinterpret_cast<T *>(static_cast<char *>(workspace) + 256);
+  a.edge_stride = (max_len + 32 + 31) / 32 * 32;
+  a.open_start = os;
+  a.open_end = oe;
+  cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
+  pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ>
+      <<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
+  return check_launch("pairwise DTW kernel");
+}
+
+template size_t pairwise_workspace_bytes<float>(uint64_t);
+template size_t pairwise_workspace_bytes<double>(uint64_t);
+template int pairwise_launch<float>(const float *, const uint64_t *, const uint64_t *, int,
+                                    uint64_t, int, int, float *, void *, size_t, cudaStream_t);
+template int pairwise_launch<double>(const double *, const uint64_t *, const uint64_t *, int,
+                                     uint64_t, int, int, double *, void *, size_t, cudaStream_t);
+
+}  // namespace odba

@@ -1,0 +1,37 @@
+// Internal declarations shared by the CUDA translation units of
+// libopendba_b200.so.  Nothing here is part of the public C ABI
+// (include/opendba_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "opendba_b200.h"
+
+namespace odba {
+
+// Records a failure in the calling thread's error slot and returns status.
+int fail(int status, const char *msg);
+// Checks cudaGetLastError() after a launch; returns ODBA_OK or ODBA_ERR_CUDA.
+int check_launch(const char *what);
+// Returns ODBA_OK if the current device is a compute capability 10.x part.
+int require_sm100();
+
+template <typename T>
+size_t pairwise_workspace_bytes(uint64_t max_len);
+template <typename T>
+int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                    uint64_t max_len, int os, int oe, T *dists, void *workspace, size_t ws_bytes,
+                    cudaStream_t stream);
+
+template <typename T>
+int medoid_launch(const T *dists, const uint64_t *lens, int n, T *sos, int *medoid,
+                  cudaStream_t stream);
+
+template <typename T>
+int znorm_launch(T *series, const uint64_t *offsets, const uint64_t *lens, int n, double *means,
+                 double *sigmas, cudaStream_t stream);
+
+}  // namespace odba

@@ -387,3 +387,94 @@ DEFINE_ORACLE(double, f64, fma, DBL_MAX)
 
 DEFINE_ZNORM(float, f32)
 DEFINE_ZNORM(double, f64)
+
+/* Distance-only restatement used as the timed CPU baseline.  Same arithmetic
+ * as sweep_*: below the top row the reference's swath-left rule equals the
+ * interior rule, so rows are one tight fused-multiply-add / min loop; the top
+ * row keeps the open-end rules.  Checked equal to oracle_pairwise_* by the tests. */
+#define DEFINE_FAST(T, SFX, FMA, FMIN, TMAX)                                                   \
+  static T fast_pair_##SFX(const T *x, size_t m, const T *y, size_t n, int os, int oe, T *prev, \
+                           T *cur) {                                                           \
+    size_t r0 = os ? 1 : 0;                                                                    \
+    T init = os ? (T)0 : TMAX;                                                                 \
+    for (size_t c = 0; c < n; ++c) prev[c] = init;                                             \
+    for (size_t r = r0; r < m; ++r) {                                                          \
+      const T xr = x[r];                                                                       \
+      T left = TMAX;                                                                           \
+      T diag = (r == 0) ? (T)0 : TMAX;                                                         \
+      if (oe && m >= 2 && r == m - 1) {                                                        \
+        for (size_t c = 0; c < n; ++c) {                                                       \
+          const T up = prev[c];                                                                \
+          const T d = xr - y[c];                                                               \
+          T v;                                                                                 \
+          if (c > 0 && c % SWATH == 0)                                                         \
+            v = FMIN(FMIN(FMA(d, d, up), diag), left);                                         \
+          else                                                                                 \
+            v = FMIN(FMA(d, d, FMIN(up, diag)), left);                                         \
+          diag = up;                                                                           \
+          left = v;                                                                            \
+          cur[c] = v;                                                                          \
+        }                                                                                      \
+      } else {                                                                                 \
+        for (size_t c = 0; c < n; ++c) {                                                       \
+          const T up = prev[c];                                                                \
+          const T d = xr - y[c];                                                               \
+          const T v = FMA(d, d, FMIN(FMIN(up, diag), left));                                   \
+          diag = up;                                                                           \
+          left = v;                                                                            \
+          cur[c] = v;                                                                          \
+        }                                                                                      \
+      }                                                                                        \
+      T *t = prev;                                                                             \
+      prev = cur;                                                                              \
+      cur = t;                                                                                 \
+    }                                                                                          \
+    return prev[n - 1];                                                                        \
+  }                                                                                            \
+                                                                                               \
+  int oracle_pairwise_fast_##SFX(const T *series, const uint64_t *offsets,                     \
+                                 const uint64_t *lens, int n, int os, int oe, T *out,          \
+                                 const int64_t *pair_list, int64_t n_list, int threads) {      \
+    int64_t npairs = (int64_t)n * (n - 1) / 2;                                                 \
+    int64_t *row_of = (int64_t *)malloc(sizeof(int64_t) * (npairs > 0 ? npairs : 1));          \
+    int64_t *col_of = (int64_t *)malloc(sizeof(int64_t) * (npairs > 0 ? npairs : 1));          \
+    int64_t p = 0;                                                                             \
+    uint64_t maxlen = 1;                                                                       \
+    for (int s = 0; s < n; ++s)                                                                \
+      if (lens[s] > maxlen) maxlen = lens[s];                                                  \
+    for (int s = 0; s + 1 < n; ++s)                                                            \
+      for (int j = s + 1; j < n; ++j) {                                                        \
+        row_of[p] = s;                                                                         \
+        col_of[p] = j;                                                                         \
+        ++p;                                                                                   \
+      }                                                                                        \
+    int64_t count = pair_list ? n_list : npairs;                                               \
+    if (threads > 0) omp_set_num_threads(threads);                                             \
+    _Pragma("omp parallel") {                                                                  \
+      T *a = (T *)malloc(sizeof(T) * maxlen);                                                  \
+      T *b = (T *)malloc(sizeof(T) * maxlen);                                                  \
+      _Pragma("omp for schedule(dynamic, 1)") for (int64_t q = 0; q < count; ++q) {            \
+        int64_t idx = pair_list ? pair_list[q] : q;                                            \
+        int64_t s = row_of[idx], j = col_of[idx];                                              \
+        size_t m = lens[s], nn = lens[j];                                                      \
+        T corner = fast_pair_##SFX(series + offsets[s], m, series + offsets[j], nn, os, oe, a, \
+                                   b);                                                         \
+        float v;                                                                               \
+        if (m == 1 && oe && !os && nn > SWATH)                                                 \
+          v = sqrtf((float)TMAX) / (float)m;                                                   \
+        else if ((oe && !os) || (!oe && os))                                                   \
+          v = sqrtf((float)corner) / (float)m;                                                 \
+        else                                                                                   \
+          v = sqrtf((float)corner);                                                            \
+        out[idx] = (T)v;                                                                       \
+      }                                                                                        \
+      free(a);                                                                                 \
+      free(b);                                                                                 \
+    }                                                                                          \
+    free(row_of);                                                                              \
+    free(col_of);                                                                              \
+    return 0;                                                                                  \
+  }
+
+DEFINE_FAST(float, f32, fmaf, fminf, FLT_MAX)
+DEFINE_FAST(double, f64, fma, fmin, DBL_MAX)

@@ -50,6 +50,15 @@ int oracle_pairwise_f64(const double *series, const uint64_t *offsets, const uin
                         int n, int open_start, int open_end, int fma_mode, double *out,
                         const int64_t *pair_list, int64_t n_list, int threads);
 
+/* Same distances as oracle_pairwise_*, distance-only tight loop (the timed
+ * CPU baseline). */
+int oracle_pairwise_fast_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                             int n, int open_start, int open_end, float *out,
+                             const int64_t *pair_list, int64_t n_list, int threads);
+int oracle_pairwise_fast_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                             int n, int open_start, int open_end, double *out,
+                             const int64_t *pair_list, int64_t n_list, int threads);
+
 /* Medoid selection of approximateMedoidIndices for one cluster (dba.hpp:186-351):
  * sums of squared distances accumulated in T in row-major pair order. */
 int oracle_medoid_f32(const float *dists, int n, const uint64_t *lens, float *sos_out);

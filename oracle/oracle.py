@@ -44,6 +44,10 @@ def lib():
             f.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P,
                           ctypes.c_int64, ctypes.c_int]
             f.restype = ctypes.c_int
+            f = getattr(_lib, f"oracle_pairwise_fast_{sfx}")
+            f.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int64,
+                          ctypes.c_int]
+            f.restype = ctypes.c_int
             f = getattr(_lib, f"oracle_medoid_{sfx}")
             f.argtypes = [P, ctypes.c_int, P, P]
             f.restype = ctypes.c_int
@@ -102,6 +106,19 @@ def pairwise(series, open_start=0, open_end=0, fma_mode=1, pair_list=None, threa
     pl = None if pair_list is None else np.ascontiguousarray(pair_list, dtype=np.int64)
     rc = getattr(lib(), f"oracle_pairwise_{_sfx(flat.dtype)}")(
         _ptr(flat), _ptr(offsets), _ptr(lens), n, open_start, open_end, fma_mode, _ptr(out),
+        _ptr(pl) if pl is not None else None, 0 if pl is None else len(pl), threads)
+    assert rc == 0
+    return out
+
+
+def pairwise_fast(series, open_start=0, open_end=0, pair_list=None, threads=0):
+    """Distance-only restatement (the timed CPU baseline); same values as pairwise()."""
+    flat, offsets, lens = pack(series)
+    n = len(series)
+    out = np.zeros(n * (n - 1) // 2, dtype=flat.dtype)
+    pl = None if pair_list is None else np.ascontiguousarray(pair_list, dtype=np.int64)
+    rc = getattr(lib(), f"oracle_pairwise_fast_{_sfx(flat.dtype)}")(
+        _ptr(flat), _ptr(offsets), _ptr(lens), n, open_start, open_end, _ptr(out),
         _ptr(pl) if pl is not None else None, 0 if pl is None else len(pl), threads)
     assert rc == 0
     return out
