@@ -60,6 +60,25 @@ int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const u
                           int n, uint64_t max_len, int use_open_start, int use_open_end,
                           double *dists, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- all-vs-all DTW distances without any device allocation -----------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory at the call site (a serving or real-time loop that forbids allocation
+ * after start-up, or a host that owns the device's whole memory budget and
+ * gives plugins no allocator): same inputs, outputs and results as
+ * odba_dtw_pairwise_f32, but the work counter and swath-edge buffers live in a
+ * fixed 64 MiB array inside the library (one per device, held while the
+ * library is loaded) instead of a caller workspace.  Limit: max_len up to
+ * 2,097,088 samples; longer series are rejected with
+ * ODBA_ERR_INVALID_ARGUMENT, and long series run with fewer warps.  The first
+ * call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialized by the caller. */
+int odba_dtw_pairwise_noalloc_f32(const float *series, const uint64_t *offsets,
+                                  const uint64_t *lens, int n, uint64_t max_len,
+                                  int use_open_start, int use_open_end, float *dists,
+                                  void *stream);
+
 /* ---- medoid from pair distances (one cluster) ------------------------------
  * Replaces the sum-of-squares and medoid choice of approximateMedoidIndices
  * (dba.hpp:186-203, 325-342).  sos (n values) and medoid (one int) are device

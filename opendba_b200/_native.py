@@ -33,6 +33,7 @@ SIGNATURES = {
     "odba_dtw_pairwise_workspace_bytes": (ctypes.c_size_t, [I32, U64]),
     "odba_dtw_pairwise_f32": (I32, [P, P, P, I32, U64, I32, I32, P, P, ctypes.c_size_t, P]),
     "odba_dtw_pairwise_f64": (I32, [P, P, P, I32, U64, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_dtw_pairwise_noalloc_f32": (I32, [P, P, P, I32, U64, I32, I32, P, P]),
     "odba_medoid_f32": (I32, [P, P, I32, P, P, P]),
     "odba_medoid_f64": (I32, [P, P, I32, P, P, P]),
     "odba_znorm_f32": (I32, [P, P, P, I32, P, P, P]),
