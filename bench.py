@@ -286,13 +286,13 @@ def main():
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
     api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)  # warm-up
     barrier(world)
-    e2e_s = []
+    e2e_s, med_e2e = [], None
     for _ in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         _, med_e2e, _, _ = api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)
         e2e_s.append(time.perf_counter() - t0)
-    e2e_sec = max_over_ranks(statistics.mean(e2e_s), world, device)
+    e2e_sec = max_over_ranks(statistics.mean(e2e_s), world, device) if e2e_s else float("nan")
     e2e_value = world * cells / e2e_sec / 1e9
     h2d = flat.nbytes + 2 * 8 * len(lens)
     d2h = npairs * 4 + 4 + 2 * 8 * len(lens)

@@ -10,9 +10,10 @@
 //
 // Layout of one swath in one warp: lane l owns the R consecutive columns
 // c0 + l*R + j (j < R), holding y[c] and the running column costs in
-// registers.  At step t lane l works on row r = r0 + t - l, so lane l needs
-// from lane l-1 the cost of the same row one column to the left (produced one
-// step earlier) -- one shuffle per step carries it.  The swath's left edge is
+// registers.  At step t lane l works on rows ra = r0 + 2(t - l) and ra + 1
+// (two interleaved dependency chains), so lane l needs from lane l-1 the costs
+// of the same two rows one column to the left (produced one step earlier) --
+// shuffles carry them, with the two x values.  The swath's left edge is
 // read from the previous swath's spilled right-edge column, the right edge is
 // spilled for the next swath.  With R = 32 a float swath is exactly the
 // reference's 1024-column swath, so the reference's swath-dependent open-end
@@ -67,35 +68,75 @@ struct SwathJob {
   T corner_init;      // diagonal input of lane 0 at its first row
 };
 
-// One wavefront step for one lane.  col[j] holds C[r-1][c_j] on entry and
-// C[r][c_j] on exit.  MASKED steps may hold lanes outside [r0, m) (fill and
-// drain of the wavefront) and the top row, where the open-end rules apply.
+// One cell: the open-end top-row rule when TOP (the right move is free,
+// dtw.hpp:196-200; at a reference swath-left column the diagonal is free too,
+// dtw.hpp:179-185), the White-Neely cost otherwise.
+template <typename T>
+__device__ __forceinline__ T cell_rule(T d, T up, T diag, T left, bool top, bool fd) {
+  const T v = Num<T>::cell(d, Num<T>::min3(up, diag, left));
+  const T vt = fd ? Num<T>::min3(Num<T>::cell(d, up), diag, left)
+                  : Num<T>::min2(Num<T>::cell(d, Num<T>::min2(up, diag)), left);
+  return top ? vt : v;
+}
+
+// Two rows per step for one lane: row a = ra and row b = ra + 1, row b one
+// column behind row a, so that the two dependency chains (left to right within
+// a row) interleave.  col[j] holds C[ra-1][c_j] on entry and C[ra+1][c_j] on
+// exit.  la / lb: costs of rows a / b one column left of the lane's first
+// column; dg: cost of row a-1 there.  Returns C[ra][c_last] (row a's last
+// column, needed by the next lane).  MASKED steps may hold lanes outside
+// [r0, m) and the top row.
 template <typename T, int R, bool MASKED>
-__device__ __forceinline__ void step_cells(T (&col)[R], const T (&yv)[R], T xin, T left, T diag,
-                                           bool active, bool top, bool free_diag0) {
+__device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T xb, T la, T lb,
+                                        T dg, bool act_a, bool act_b, bool top_a, bool top_b,
+                                        bool fd0) {
+  T a_left = la, a_diag = dg;
+  T b_left = lb, b_diag = la;
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const T up = col[j];
-    const T d = xin - yv[j];
-    T v = Num<T>::cell(d, Num<T>::min3(up, diag, left));
+    const T da = xa - yv[j];
+    T va;
     if (MASKED) {
-      // top row with open end: the right move is free (dtw.hpp:196-200); at a
-      // reference swath-left column the diagonal is free too (dtw.hpp:179-185)
-      T vt = (j == 0 && free_diag0) ? Num<T>::min3(Num<T>::cell(d, up), diag, left)
-                                    : Num<T>::min2(Num<T>::cell(d, Num<T>::min2(up, diag)), left);
-      v = top ? vt : v;
-      v = active ? v : up;
+      va = cell_rule<T>(da, up, a_diag, a_left, top_a, j == 0 && fd0);
+      va = act_a ? va : up;
+    } else {
+      va = Num<T>::cell(da, Num<T>::min3(up, a_diag, a_left));
     }
-    diag = up;
-    left = v;
-    col[j] = v;
+    a_diag = up;
+    a_left = va;
+    const T db = xb - yv[j];
+    T vb;
+    if (MASKED) {
+      vb = cell_rule<T>(db, va, b_diag, b_left, top_b, j == 0 && fd0);
+      vb = act_b ? vb : va;
+    } else {
+      vb = Num<T>::cell(db, Num<T>::min3(va, b_diag, b_left));
+    }
+    b_diag = va;
+    b_left = vb;
+    col[j] = vb;
   }
+  return a_left;
 }
 
+template <typename T>
+struct Pair2;
+template <>
+struct Pair2<float> {
+  using V = float2;
+};
+template <>
+struct Pair2<double> {
+  using V = double2;
+};
+
 // Sweeps one swath.  On return col[] holds, per lane, the costs of the last
-// row m-1 at the lane's columns (rows beyond m-1 are never applied).
+// row m-1 at the lane's columns.  Swath-edge buffers are indexed by r - r0,
+// two rows per 8/16-byte access.
 template <typename T, int R>
 __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R]) {
+  using V2 = typename Pair2<T>::V;
   const int lane = threadIdx.x & 31;
   const int m = job.m;
   const int r0 = job.r0;
@@ -113,81 +154,84 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R])
 
   const bool has_in = job.edge_in != nullptr;
   const bool has_out = job.edge_out != nullptr;
-  const int total = (m - r0) + 31;  // wavefront steps including fill and drain
+  const int rows = m - r0;
+  const int total = (rows + 1) / 2 + 31;  // wavefront steps including fill and drain
   const bool lane0 = lane == 0, lane31 = lane == 31;
   const bool oe_top = job.open_end && m >= 2;  // a single-row matrix has no open-end rule
   const bool fd0 = job.free_diag0 && lane0;
+  const int last_x = m - 1, last_e = rows > 0 ? rows - 1 : 0;
 
-  T xcur = T(0);
-  T left_prev = lane0 ? job.corner_init : init;
+  T xa_cur = T(0), xb_cur = T(0), a_last = init;
+  T dg = lane0 ? job.corner_init : init;
 
-  auto lane0_inputs = [&](int r, T &x, T &e) {
-    const int rc = r < m ? r : m - 1;
-    x = job.x[rc];
-    e = has_in ? job.edge_in[rc] : Num<T>::big();
+  // lane 0's inputs of step t: x of rows a, b and the left-edge costs of rows a, b
+  auto fetch = [&](int t, T &xa, T &xb, T &ea, T &eb) {
+    const int k = 2 * t;  // ra - r0
+    const int ka = k < last_e ? k : last_e, kb = k + 1 < last_e ? k + 1 : last_e;
+    const int ia = r0 + k < last_x ? r0 + k : last_x;
+    const int ib = r0 + k + 1 < last_x ? r0 + k + 1 : last_x;
+    xa = job.x[ia];
+    xb = job.x[ib];
+    if (has_in) {
+      ea = job.edge_in[ka];
+      eb = job.edge_in[kb];
+    } else {
+      ea = eb = Num<T>::big();
+    }
   };
 
   auto masked_step = [&](int t) {
-    const int r = r0 + t - lane;
-    T xin = __shfl_up_sync(kFull, xcur, 1);
-    T lin = __shfl_up_sync(kFull, col[R - 1], 1);
-    if (lane0) lane0_inputs(r, xin, lin);
-    const T diag = left_prev;
-    left_prev = lin;
-    xcur = xin;
-    const bool active = (r >= r0) && (r < m);
-    const bool top = oe_top && (r == m - 1);
-    step_cells<T, R, true>(col, yv, xin, lin, diag, active, top, fd0);
-    if (lane31 && has_out && active) job.edge_out[r] = col[R - 1];
+    const int ra = r0 + 2 * (t - lane);
+    T xa = __shfl_up_sync(kFull, xa_cur, 1);
+    T xb = __shfl_up_sync(kFull, xb_cur, 1);
+    T la = __shfl_up_sync(kFull, a_last, 1);
+    T lb = __shfl_up_sync(kFull, col[R - 1], 1);
+    if (lane0) fetch(t, xa, xb, la, lb);
+    const T diag = dg;
+    dg = lb;
+    const bool act_a = ra >= r0 && ra < m, act_b = ra + 1 >= r0 && ra + 1 < m;
+    a_last = step_rows2<T, R, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
+                                    oe_top && ra == m - 1, oe_top && ra + 1 == m - 1, fd0);
+    xa_cur = xa;
+    xb_cur = xb;
+    if (lane31 && has_out) {
+      if (act_a) job.edge_out[ra - r0] = a_last;
+      if (act_b) job.edge_out[ra + 1 - r0] = col[R - 1];
+    }
   };
 
-  const int steady_end = (m - 1 - r0) > 31 ? (m - 1 - r0) : 31;
+  // steady state: rows a, b of every lane in [r0, m-2]
+  int steady_end = (rows - 1) / 2;  // first step at which lane 0's row b reaches m-1
+  if (steady_end < 31) steady_end = 31;
   const int fill_end = total < 31 ? total : 31;
   int t = 0;
   for (; t < fill_end; ++t) masked_step(t);
-
-  // Steady state: every lane holds a row in [r0, m-2]; no masks, no top row.
-  // Lane 0's inputs are prefetched four steps ahead.
-  if (t + 4 <= steady_end) {
-    T qx[4], qe[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      qx[k] = T(0);
-      qe[k] = T(0);
-    }
-    if (lane0) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) lane0_inputs(r0 + t + k, qx[k], qe[k]);
-    }
-    for (; t + 4 <= steady_end; t += 4) {
-      T nx[4], ne[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        nx[k] = T(0);
-        ne[k] = T(0);
-      }
+  if (t < steady_end) {
+    T pxa = T(0), pxb = T(0), pea = T(0), peb = T(0);
+    if (lane0) fetch(t, pxa, pxb, pea, peb);
+    for (; t < steady_end; ++t) {
+      T xa = __shfl_up_sync(kFull, xa_cur, 1);
+      T xb = __shfl_up_sync(kFull, xb_cur, 1);
+      T la = __shfl_up_sync(kFull, a_last, 1);
+      T lb = __shfl_up_sync(kFull, col[R - 1], 1);
       if (lane0) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) lane0_inputs(r0 + t + 4 + k, nx[k], ne[k]);
+        xa = pxa;
+        xb = pxb;
+        la = pea;
+        lb = peb;
+        fetch(t + 1, pxa, pxb, pea, peb);
       }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        T xin = __shfl_up_sync(kFull, xcur, 1);
-        T lin = __shfl_up_sync(kFull, col[R - 1], 1);
-        if (lane0) {
-          xin = qx[k];
-          lin = qe[k];
-        }
-        const T diag = left_prev;
-        left_prev = lin;
-        xcur = xin;
-        step_cells<T, R, false>(col, yv, xin, lin, diag, true, false, false);
-        if (lane31 && has_out) job.edge_out[r0 + t + k - 31] = col[R - 1];
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        qx[k] = nx[k];
-        qe[k] = ne[k];
+      const T diag = dg;
+      dg = lb;
+      a_last = step_rows2<T, R, false>(col, yv, xa, xb, la, lb, diag, true, true, false, false,
+                                       false);
+      xa_cur = xa;
+      xb_cur = xb;
+      if (lane31 && has_out) {
+        V2 v;
+        v.x = a_last;
+        v.y = col[R - 1];
+        *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
       }
     }
   }

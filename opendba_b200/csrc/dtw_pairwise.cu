@@ -25,6 +25,7 @@ namespace odba {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
+constexpr int kMinBlocksPerSM = 3;  // 12 warps per SM measured fastest (16 is slower, 20 spills)
 
 template <typename T>
 struct PairwiseArgs {
@@ -121,7 +122,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
 }
 
 template <typename T, int RF, int RQ>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     pairwise_kernel(PairwiseArgs<T> a) {
   const int lane = threadIdx.x & 31;
   const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
