@@ -96,6 +96,33 @@ int odba_znorm_f32(float *series, const uint64_t *offsets, const uint64_t *lens,
 int odba_znorm_f64(double *series, const uint64_t *offsets, const uint64_t *lens, int n,
                    double *means, double *sigmas, void *stream);
 
+/* ---- one DBA round -------------------------------------------------------------
+ * Replaces DBAUpdate<T> (dba.hpp:432-848) with updateCentroid (dba.hpp:374-423)
+ * for the full-path (non-stripe) case: aligns every member to the centroid by
+ * DTW with a recorded path, backtracks, and averages the aligned member samples
+ * into new_centroid (Lc values, T) with their pile-up counts; *delta (device
+ * double) receives max |centroid - new_centroid|.  Members are processed in the
+ * given order, and every centroid sum is added in the reference's order, so
+ * the result is bit-identical to the reference's.  h_lens is a host copy of
+ * lens (it sizes the workspace).  If path_triples is non-NULL it receives, per
+ * member k starting at triple sum_{i<k}(lens[i] + Lc + 1), the path as
+ * (row, column, move) int32 triples in the order of the reference's path file
+ * (io_utils.hpp:287-323, move codes of dtw.hpp:10-16), and path_counts[k] the
+ * number of triples (-1 if the walk failed). */
+size_t odba_dba_round_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
+                                      uint64_t centroid_len, int use_open_start, int use_open_end);
+int odba_dba_round_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                       const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                       int use_open_start, int use_open_end, float *new_centroid, uint32_t *counts,
+                       double *delta, int32_t *path_triples, int64_t *path_counts,
+                       void *workspace, size_t workspace_bytes, void *stream);
+int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                       const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                       int use_open_start, int use_open_end, double *new_centroid,
+                       uint32_t *counts, double *delta, int32_t *path_triples,
+                       int64_t *path_counts, void *workspace, size_t workspace_bytes,
+                       void *stream);
+
 /* ---- host-buffer medoid pass (end to end) ------------------------------------
  * What performDBA does between its sort and the DBA rounds for one cluster
  * (dba.hpp:902-928 with approximateMedoidIndices): copies the concatenated

@@ -142,3 +142,47 @@ def medoid_pass_host(series, open_start: int = 0, open_end: int = 0, norm: int =
                  n, int(open_start), int(open_end), int(norm), vp(dists_out), vp(med),
                  vp(means), vp(sigmas), stream)
     return dists_out[:npairs], int(med[0]), means, sigmas
+
+
+def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: int = 0,
+              with_paths: bool = False, workspace=None, stream=None):
+    """One DBA round of ``members`` against ``centroid`` (DBAUpdate, dba.hpp:434).
+
+    centroid: device tensor (same dtype as members).  Returns (new_centroid,
+    counts, delta, paths) where paths is None or a list of (k, 3) int32 numpy
+    arrays (row, column, move) in the order of the reference's path files."""
+    torch = _torch()
+    Lc = int(centroid.numel())
+    dev = members.data.device
+    lib = _native.lib()
+    h_lens = np.ascontiguousarray(members.host_lens, dtype=np.uint64)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    if workspace is None:
+        nbytes = lib.odba_dba_round_workspace_bytes(members.dtype.itemsize, vp(h_lens), members.n,
+                                                    Lc, int(open_start), int(open_end))
+        workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    mean = torch.empty(Lc, dtype=members.data.dtype, device=dev)
+    counts = torch.empty(Lc, dtype=torch.int32, device=dev)
+    delta = torch.empty(1, dtype=torch.float64, device=dev)
+    tri = cnt = None
+    if with_paths:
+        cap = int(h_lens.sum()) + members.n * (Lc + 1)
+        tri = torch.empty(3 * cap, dtype=torch.int32, device=dev)
+        cnt = torch.empty(members.n, dtype=torch.int64, device=dev)
+    _native.call(f"odba_dba_round_{_SFX[members.dtype]}", centroid.data_ptr(), Lc,
+                 members.data.data_ptr(), members.offsets.data_ptr(), members.lens.data_ptr(),
+                 vp(h_lens), members.n, int(open_start), int(open_end), mean.data_ptr(),
+                 counts.data_ptr(), delta.data_ptr(), tri.data_ptr() if tri is not None else None,
+                 cnt.data_ptr() if cnt is not None else None, workspace.data_ptr(),
+                 workspace.numel(), _stream_ptr(stream))
+    paths = None
+    if with_paths:
+        t = tri.cpu().numpy()
+        c = cnt.cpu().numpy()
+        paths, pos = [], 0
+        for k in range(members.n):
+            if c[k] < 0:
+                raise _native.OdbaError(2, f"backtrack of member {k} failed")
+            paths.append(t[3 * pos:3 * (pos + int(c[k]))].reshape(-1, 3))
+            pos += int(h_lens[k]) + Lc + 1
+    return mean, counts.view(torch.int32), float(delta.item()), paths

@@ -134,6 +134,27 @@ int medoid_pass_host(const T *h_series, const uint64_t *h_lens, int n, int os, i
   return rc;
 }
 
+template <typename T>
+int dba_round_checked(const T *centroid, uint64_t Lc, const T *series,
+                             const uint64_t *offsets, const uint64_t *lens,
+                             const uint64_t *h_lens, int n, int os, int oe, T *mean,
+                             uint32_t *counts, double *delta, int32_t *triples,
+                             int64_t *triple_counts, void *ws, size_t ws_bytes, void *stream) {
+  if (n < 1 || Lc == 0 || !centroid || !series || !offsets || !lens || !h_lens || !mean ||
+      !counts || !delta || !ws)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer, empty centroid or no members");
+  if ((triples == nullptr) != (triple_counts == nullptr))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "path triples and their counts go together");
+  for (int k = 0; k < n; ++k)
+    if (h_lens[k] == 0 || h_lens[k] > (1ull << 30))
+      return fail(ODBA_ERR_INVALID_ARGUMENT, "member lengths must be in [1, 2^30]");
+  if (Lc > (1ull << 30)) return fail(ODBA_ERR_INVALID_ARGUMENT, "centroid too long");
+  if (int rc = require_sm100()) return rc;
+  return dba_round_launch<T>(centroid, Lc, series, offsets, lens, h_lens, n, os ? 1 : 0,
+                             oe ? 1 : 0, mean, counts, delta, triples, triple_counts, ws,
+                             ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
 }  // namespace
 }  // namespace odba
 
@@ -224,6 +245,35 @@ int odba_medoid_pass_host_f64(const double *h_series, const uint64_t *h_lens, in
                               int *h_medoid, double *h_means, double *h_sigmas, void *stream) {
   return medoid_pass_host<double>(h_series, h_lens, n, use_open_start, use_open_end, norm, h_dists,
                                   h_medoid, h_means, h_sigmas, stream);
+}
+
+size_t odba_dba_round_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
+                                      uint64_t centroid_len, int use_open_start, int use_open_end) {
+  if (n < 1 || !h_lens || centroid_len == 0) return 0;
+  if (elem_size == 8)
+    return dba_round_workspace_bytes<double>(h_lens, n, centroid_len, use_open_start, use_open_end);
+  return dba_round_workspace_bytes<float>(h_lens, n, centroid_len, use_open_start, use_open_end);
+}
+
+int odba_dba_round_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                       const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                       int use_open_start, int use_open_end, float *new_centroid, uint32_t *counts,
+                       double *delta, int32_t *path_triples, int64_t *path_counts,
+                       void *workspace, size_t workspace_bytes, void *stream) {
+  return dba_round_checked<float>(centroid, centroid_len, series, offsets, lens, h_lens, n,
+                                  use_open_start, use_open_end, new_centroid, counts, delta,
+                                  path_triples, path_counts, workspace, workspace_bytes, stream);
+}
+
+int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                       const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                       int use_open_start, int use_open_end, double *new_centroid,
+                       uint32_t *counts, double *delta, int32_t *path_triples,
+                       int64_t *path_counts, void *workspace, size_t workspace_bytes,
+                       void *stream) {
+  return dba_round_checked<double>(centroid, centroid_len, series, offsets, lens, h_lens, n,
+                                   use_open_start, use_open_end, new_centroid, counts, delta,
+                                   path_triples, path_counts, workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -1,0 +1,167 @@
+// Path-recording variant of the swath sweep in dtw_device.cuh, for the DBA
+// round (DBAUpdate's DTWDistance launches with a path matrix, dba.hpp:589-617).
+//
+// Each cell also records the reference's move choice (dtw.hpp:202-227):
+//   if (diag > up) move = (up > right) ? RIGHT : UP
+//   else           move = (diag > right) ? RIGHT : DIAGONAL
+// over the three candidate costs rounded separately (fma(d, d, pred), or the
+// free predecessor on the open-end top row).  Ties therefore resolve
+// DIAGONAL > UP > RIGHT, i.e. move = DIAGONAL if diag == min, else UP if
+// up == min, else RIGHT.  Moves are 2-bit codes (1 DIAGONAL, 2 RIGHT, 3 UP);
+// the codes the reference derives from position alone (row 0, (0, 0), the
+// open-end OPEN_RIGHT) are rebuilt by the backtrack.
+//
+// Path layout per swath: step t, lane l, row slot s (0 = row a, 1 = row b)
+// at 64-bit word ((t * 32 + l) * 2 + s); bit pair 2j holds register j's move.
+// A warp writes 512 contiguous bytes per step.
+#pragma once
+
+#include "dtw_device.cuh"
+
+namespace odba {
+
+// One cell with its move.  top: open-end top row (right free); fd: the
+// reference's swath-left column on that row (diagonal free too).
+template <typename T, bool MASKED>
+__device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool fd,
+                                       unsigned &code) {
+  const T uv = Num<T>::cell(d, up);
+  T dv = Num<T>::cell(d, diag);
+  T rv = Num<T>::cell(d, left);
+  if (MASKED) {
+    rv = top ? left : rv;
+    dv = (top && fd) ? diag : dv;
+  }
+  const T v = Num<T>::min3(uv, dv, rv);
+  code = (dv == v) ? 1u : ((uv == v) ? 3u : 2u);
+  return v;
+}
+
+template <typename T, int R, bool MASKED>
+__device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa, T xb, T la,
+                                             T lb, T dg, bool act_a, bool act_b, bool top_a,
+                                             bool top_b, bool fd0, unsigned long long &wa,
+                                             unsigned long long &wb) {
+  T a_left = la, a_diag = dg;
+  T b_left = lb, b_diag = la;
+  wa = 0ull;
+  wb = 0ull;
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const T up = col[j];
+    unsigned ca, cb;
+    T va = path_cell<T, MASKED>(xa - yv[j], up, a_diag, a_left, top_a, j == 0 && fd0, ca);
+    if (MASKED) va = act_a ? va : up;
+    a_diag = up;
+    a_left = va;
+    T vb = path_cell<T, MASKED>(xb - yv[j], va, b_diag, b_left, top_b, j == 0 && fd0, cb);
+    if (MASKED) vb = act_b ? vb : va;
+    b_diag = va;
+    b_left = vb;
+    col[j] = vb;
+    wa |= (unsigned long long)ca << (2 * j);
+    wb |= (unsigned long long)cb << (2 * j);
+  }
+  return a_left;
+}
+
+struct PathOut {
+  unsigned long long *words;  // this swath's move words, (steps * 32 * 2) of them
+  bool track_min;             // record min / top of this swath's right-edge column
+};
+
+// Sweeps one swath recording moves.  Same wavefront as sweep_swath; in
+// addition lane 31 keeps the minimum of the right-edge column it spills and
+// its top-row value (for the reference's open-end shortcut, dtw.hpp:74-129).
+template <typename T, int R>
+__device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const PathOut &po,
+                                                 T (&col)[R], T &edge_min, T &edge_top) {
+  const int lane = threadIdx.x & 31;
+  const int m = job.m;
+  const int r0 = job.r0;
+  T yv[R];
+  {
+    const int cl = job.c0 + lane * R;
+#pragma unroll
+    for (int j = 0; j < R; ++j) yv[j] = (cl + j < job.n) ? job.y[cl + j] : T(0);
+  }
+  const T init = r0 ? T(0) : Num<T>::big();
+#pragma unroll
+  for (int j = 0; j < R; ++j) col[j] = init;
+
+  const bool has_in = job.edge_in != nullptr;
+  const bool has_out = job.edge_out != nullptr;
+  const int rows = m - r0;
+  const int total = (rows + 1) / 2 + 31;
+  const bool lane0 = lane == 0, lane31 = lane == 31;
+  const bool oe_top = job.open_end && m >= 2;
+  const bool fd0 = job.free_diag0 && lane0;
+  const int last_x = m - 1, last_e = rows > 0 ? rows - 1 : 0;
+  T emin = Num<T>::big(), etop = Num<T>::big();
+
+  T xa_cur = T(0), xb_cur = T(0), a_last = init;
+  T dg = lane0 ? job.corner_init : init;
+
+  auto fetch = [&](int t, T &xa, T &xb, T &ea, T &eb) {
+    const int k = 2 * t;
+    const int ka = k < last_e ? k : last_e, kb = k + 1 < last_e ? k + 1 : last_e;
+    const int ia = r0 + k < last_x ? r0 + k : last_x;
+    const int ib = r0 + k + 1 < last_x ? r0 + k + 1 : last_x;
+    xa = job.x[ia];
+    xb = job.x[ib];
+    if (has_in) {
+      ea = job.edge_in[ka];
+      eb = job.edge_in[kb];
+    } else {
+      ea = eb = Num<T>::big();
+    }
+  };
+
+  auto store_words = [&](int t, unsigned long long wa, unsigned long long wb) {
+    ulonglong2 w;
+    w.x = wa;
+    w.y = wb;
+    reinterpret_cast<ulonglong2 *>(po.words)[t * 32 + lane] = w;
+  };
+
+  for (int t = 0; t < total; ++t) {
+    const int ra = r0 + 2 * (t - lane);
+    T xa = __shfl_up_sync(kFull, xa_cur, 1);
+    T xb = __shfl_up_sync(kFull, xb_cur, 1);
+    T la = __shfl_up_sync(kFull, a_last, 1);
+    T lb = __shfl_up_sync(kFull, col[R - 1], 1);
+    if (lane0) fetch(t, xa, xb, la, lb);
+    const T diag = dg;
+    dg = lb;
+    const bool act_a = ra >= r0 && ra < m, act_b = ra + 1 >= r0 && ra + 1 < m;
+    unsigned long long wa, wb;
+    const bool interior = (t >= 31) && (2 * t + 1 < rows - 1);
+    if (interior) {
+      a_last = step_rows2_path<T, R, false>(col, yv, xa, xb, la, lb, diag, true, true, false,
+                                            false, false, wa, wb);
+    } else {
+      a_last = step_rows2_path<T, R, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
+                                           oe_top && ra == m - 1, oe_top && ra + 1 == m - 1, fd0,
+                                           wa, wb);
+    }
+    xa_cur = xa;
+    xb_cur = xb;
+    store_words(t, wa, wb);
+    if (lane31) {
+      if (act_a) {
+        if (has_out) job.edge_out[ra - r0] = a_last;
+        emin = Num<T>::min2(emin, a_last);
+        if (ra == m - 1) etop = a_last;
+      }
+      if (act_b) {
+        if (has_out) job.edge_out[ra + 1 - r0] = col[R - 1];
+        emin = Num<T>::min2(emin, col[R - 1]);
+        if (ra + 1 == m - 1) etop = col[R - 1];
+      }
+    }
+  }
+  edge_min = __shfl_sync(kFull, emin, 31);
+  edge_top = __shfl_sync(kFull, etop, 31);
+}
+
+}  // namespace odba

@@ -34,4 +34,12 @@ template <typename T>
 int znorm_launch(T *series, const uint64_t *offsets, const uint64_t *lens, int n, double *means,
                  double *sigmas, cudaStream_t stream);
 
+template <typename T>
+size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe);
+template <typename T>
+int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint64_t *offsets,
+                     const uint64_t *lens, const uint64_t *h_lens, int n, int os, int oe, T *mean,
+                     uint32_t *counts, double *delta, int32_t *triples, int64_t *triple_counts,
+                     void *ws, size_t ws_bytes, cudaStream_t stream);
+
 }  // namespace odba

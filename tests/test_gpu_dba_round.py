@@ -1,0 +1,98 @@
+"""Parity of the CUDA DBA round (path DTW, backtrack, ordered centroid update).
+
+Bit-exact against the reference's own GPU round (tests/golden/ref/dba_*: the
+updated centroid, the delta and every member's path) and against the CPU
+oracle on seeded random cases, including the open-end shortcut and flipped
+(centroid-on-rows) members, through the C ABI.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MODES = {"global": (0, 0), "open_start": (1, 0), "open_end": (0, 1), "open": (1, 1)}
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from opendba_b200 import api, build
+    build.build_library()
+    return torch, api
+
+
+def _bits(a):
+    a = np.asarray(a)
+    return a.view(np.uint32 if a.dtype == np.float32 else np.uint64)
+
+
+def _round(env, centroid, members, os_, oe, with_paths=True):
+    torch, api = env
+    ds = api.DeviceSeries.from_host(members)
+    c = torch.from_numpy(np.ascontiguousarray(centroid)).cuda()
+    mean, counts, delta, paths = api.dba_round(c, ds, os_, oe, with_paths=with_paths)
+    return mean.cpu().numpy(), counts.cpu().numpy(), delta, paths
+
+
+@pytest.mark.parametrize("sfx", ["f32", "f64"])
+@pytest.mark.parametrize("mode", list(MODES))
+def test_round_matches_reference_gpu(env, sfx, mode):
+    members = O.read_bundle(os.path.join(GOLDEN, f"dba_{sfx}_members.odbs"))
+    centroid = O.read_bundle(os.path.join(GOLDEN, f"dba_{sfx}_centroid.odbs"))[0]
+    ref = O.read_bundle(os.path.join(GOLDEN, f"dba_{sfx}_{mode}.mean.odbs"))[0]
+    with open(os.path.join(GOLDEN, f"dba_{sfx}_{mode}.delta.txt")) as f:
+        ref_delta = float(f.read())
+    os_, oe = MODES[mode]
+    mean, counts, delta, paths = _round(env, centroid, members, os_, oe)
+    assert np.array_equal(_bits(mean), _bits(ref))
+    assert delta == ref_delta
+    gold = np.load(os.path.join(GOLDEN, f"dba_{sfx}_{mode}.paths.npz"))
+    for k, seq in enumerate(members):
+        ij = gold[f"ij{k}"].copy()
+        if oe and len(centroid) < len(seq):
+            ij[:-1] = ij[:-1, ::-1]  # flipped members print "column, row"
+        assert np.array_equal(paths[k][:, :2], ij), f"member {k} path cells"
+        assert np.array_equal(paths[k][:, 2].astype(np.uint8), gold[f"mv{k}"]), f"member {k} moves"
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("mode", list(MODES))
+def test_round_random_vs_oracle(env, dtype, mode):
+    rng = np.random.default_rng(99 + list(MODES).index(mode))
+    os_, oe = MODES[mode]
+    # centroid 1500 > 1024: two swaths; members shorter (shortcut candidates
+    # in open_end) and longer (flipped in open_end), ragged
+    lens = [3, 40, 700, 1023, 1024, 1025, 1499, 1500, 1501, 2100, 3300, 500]
+    members = [np.cumsum(rng.standard_normal(L)).astype(dtype) for L in lens]
+    centroid = np.cumsum(rng.standard_normal(1500)).astype(dtype)
+    mean, counts, delta, paths = _round(env, centroid, members, os_, oe)
+    w_mean, w_counts, _, w_delta = O.dba_update(centroid, members, os_, oe, fma_mode=1)
+    assert np.array_equal(_bits(mean), _bits(w_mean))
+    assert np.array_equal(counts.astype(np.uint32), w_counts)
+    assert delta == w_delta
+    for k, seq in enumerate(members):
+        t = O.path_triples(centroid, seq, os_, oe, fma_mode=1)
+        assert np.array_equal(paths[k], t.astype(np.int32)), f"member {k}"
+
+
+def test_round_open_end_shortcut_fires(env):
+    # a short member against a long flat centroid: the top row becomes the
+    # column minimum early, so the reference's shortcut decides the path end
+    rng = np.random.default_rng(5)
+    centroid = np.concatenate([np.cumsum(rng.standard_normal(300)), np.zeros(3000)]).astype(np.float32)
+    members = [centroid[:300].copy() + 0.01 * rng.standard_normal(300).astype(np.float32),
+               centroid[:250].copy()]
+    mean, counts, delta, paths = _round(env, centroid, members, 0, 1)
+    w_mean, w_counts, _, w_delta = O.dba_update(centroid, members, 0, 1, fma_mode=1)
+    assert np.array_equal(_bits(mean), _bits(w_mean))
+    for k, seq in enumerate(members):
+        t = O.path_triples(centroid, seq, 0, 1, fma_mode=1)
+        assert np.array_equal(paths[k], t.astype(np.int32))
+        assert (paths[k][:, 2] == 4).sum() > 1000  # a long OPEN_RIGHT run on the top row
