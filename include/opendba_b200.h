@@ -123,6 +123,25 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
                        int64_t *path_counts, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* ---- k-segmentation ------------------------------------------------------------
+ * Replaces the kernel part of adaptive_segmentation<T> (adaptive_device_segmentation,
+ * segmentation.hpp:48-337; launch segmentation.hpp:440-463).  Every block of
+ * 256*ceil(min_segment_length/3) samples of every series gets k_max median slots
+ * (k_max = ceil(256 / (min_segment_length / ceil(min_segment_length/3))) as the
+ * reference computes it); unused slots hold the type's max.  medians must hold
+ * odba_segment_capacity(h_lens, n, min_segment_length) values, series first, then
+ * blocks in order.  The host-side merge of block edges and sentinel removal
+ * (segmentation.hpp:486-578) is done by adaptive_segmentation<T> in opendba.hpp.
+ * The workspace holds n 64-bit offsets. */
+size_t odba_segment_capacity(const uint64_t *h_lens, int n, int min_segment_length);
+size_t odba_segment_workspace_bytes(int n);
+int odba_segment_blocks_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                            const uint64_t *h_lens, int n, int min_segment_length, float *medians,
+                            void *workspace, size_t workspace_bytes, void *stream);
+int odba_segment_blocks_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                            const uint64_t *h_lens, int n, int min_segment_length, double *medians,
+                            void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- host-buffer medoid pass (end to end) ------------------------------------
  * What performDBA does between its sort and the DBA rounds for one cluster
  * (dba.hpp:902-928 with approximateMedoidIndices): copies the concatenated
@@ -136,6 +155,36 @@ int odba_medoid_pass_host_f32(const float *h_series, const uint64_t *h_lens, int
 int odba_medoid_pass_host_f64(const double *h_series, const uint64_t *h_lens, int n,
                               int use_open_start, int use_open_end, int norm, double *h_dists,
                               int *h_medoid, double *h_means, double *h_sigmas, void *stream);
+
+/* ---- whole pipeline (the C++ façade in opendba.hpp, callable over FFI) --------
+ * odba_perform_dba_*: performDBA<T> (dba.hpp:863-1189) on host series
+ * (sorted, z-normalised and truncated in place like the reference does), with
+ * algo_mode CLUSTER_ONLY (1), CONSENSUS_ONLY (2) or CLUSTER_AND_CONSENSUS (3);
+ * writes <prefix>.pair_dists.txt, <prefix>.avg.txt, per-cluster path and
+ * checkpoint files.  odba_setup_and_run: setupAndRun<T> (openDBA.cuh:13-200)
+ * for elem_size 4 (float) or 8 (double): reads text / binary / TSV files,
+ * optionally segments them, then runs performDBA.  Like the reference, these
+ * end the process with its exit codes (exit_codes.hpp) on fatal input/output
+ * errors; otherwise they return ODBA_OK.
+ * odba_segment_host_*: adaptive_segmentation<T> (segmentation.hpp:340-583) on
+ * concatenated host series; h_out needs odba_segment_capacity(...) values and
+ * receives each series' segment medians back to back, h_out_lens the counts. */
+int odba_perform_dba_f32(float **sequences, int num_sequences, size_t *lengths, char **names,
+                         int use_open_start, int use_open_end, const char *output_prefix,
+                         int norm, double cdist, int algo_mode);
+int odba_perform_dba_f64(double **sequences, int num_sequences, size_t *lengths, char **names,
+                         int use_open_start, int use_open_end, const char *output_prefix,
+                         int norm, double cdist, int algo_mode);
+int odba_setup_and_run(int elem_size, const char *seqprefix_file, char **files, int num_files,
+                       const char *output_prefix, int read_mode, int use_open_start,
+                       int use_open_end, const char *min_segment_length, int norm, double cdist,
+                       int prefix_start, int prefix_length, int is_short);
+int odba_segment_host_f32(const float *h_series, const uint64_t *h_lens, int n,
+                          int min_segment_length, int prefix_skip, float *h_out,
+                          uint64_t *h_out_lens);
+int odba_segment_host_f64(const double *h_series, const uint64_t *h_lens, int n,
+                          int min_segment_length, int prefix_skip, double *h_out,
+                          uint64_t *h_out_lens);
 
 #ifdef __cplusplus
 }

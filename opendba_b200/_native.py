@@ -43,6 +43,18 @@ SIGNATURES = {
                                  ctypes.c_size_t, P]),
     "odba_dba_round_f64": (I32, [P, U64, P, P, P, P, I32, I32, I32, P, P, P, P, P, P,
                                  ctypes.c_size_t, P]),
+    "odba_segment_capacity": (ctypes.c_size_t, [P, I32, I32]),
+    "odba_segment_workspace_bytes": (ctypes.c_size_t, [I32]),
+    "odba_segment_blocks_f32": (I32, [P, P, P, P, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_segment_blocks_f64": (I32, [P, P, P, P, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_perform_dba_f32": (I32, [P, I32, P, P, I32, I32, ctypes.c_char_p, I32, ctypes.c_double,
+                                   I32]),
+    "odba_perform_dba_f64": (I32, [P, I32, P, P, I32, I32, ctypes.c_char_p, I32, ctypes.c_double,
+                                   I32]),
+    "odba_setup_and_run": (I32, [I32, ctypes.c_char_p, P, I32, ctypes.c_char_p, I32, I32, I32,
+                                 ctypes.c_char_p, I32, ctypes.c_double, I32, I32, I32]),
+    "odba_segment_host_f32": (I32, [P, P, I32, I32, I32, P, P]),
+    "odba_segment_host_f64": (I32, [P, P, I32, I32, I32, P, P]),
     "odba_medoid_pass_host_f32": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
     "odba_medoid_pass_host_f64": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
 }

@@ -186,3 +186,53 @@ def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: in
             paths.append(t[3 * pos:3 * (pos + int(c[k]))].reshape(-1, 3))
             pos += int(h_lens[k]) + Lc + 1
     return mean, counts.view(torch.int32), float(delta.item()), paths
+
+
+def perform_dba(series, names, output_prefix: str, open_start: int = 0, open_end: int = 0,
+                norm: int = 1, cdist: float = 1.0, algo_mode: int = 3):
+    """performDBA<T> (dba.hpp:863) on host series: writes the reference's
+    output files under ``output_prefix``.  Ends the process on the reference's
+    fatal errors, like the reference does."""
+    dt = np.dtype(np.asarray(series[0]).dtype)
+    arrs = [np.ascontiguousarray(s, dtype=dt) for s in series]
+    n = len(arrs)
+    ptrs = (ctypes.c_void_p * n)(*[a.ctypes.data for a in arrs])
+    lens = (ctypes.c_size_t * n)(*[len(a) for a in arrs])
+    cnames = [ctypes.create_string_buffer(str(nm).encode()) for nm in names]
+    name_ptrs = (ctypes.c_char_p * n)(*[ctypes.addressof(c) for c in cnames])
+    _native.call(f"odba_perform_dba_{_SFX[dt]}", ptrs, n, lens, name_ptrs, int(open_start),
+                 int(open_end), output_prefix.encode(), int(norm), float(cdist), int(algo_mode))
+    return [a for a in arrs]
+
+
+def setup_and_run(files, output_prefix: str, read_mode: int = 0, open_start: int = 0,
+                  open_end: int = 0, min_segment_length: str = "0", norm: int = 1,
+                  cdist: float = 1.0, dtype=np.float32, seqprefix_file=None, prefix_start: int = 0,
+                  prefix_length: int = 0, is_short: bool = False):
+    """setupAndRun<T> (openDBA.cuh:15): read_mode 0 text, 1 binary, 2 TSV."""
+    n = len(files)
+    bufs = [ctypes.create_string_buffer(f.encode()) for f in files]
+    arr = (ctypes.c_char_p * n)(*[ctypes.addressof(b) for b in bufs])
+    _native.call("odba_setup_and_run", np.dtype(dtype).itemsize,
+                 seqprefix_file.encode() if seqprefix_file else None, arr, n,
+                 output_prefix.encode(), int(read_mode), int(open_start), int(open_end),
+                 str(min_segment_length).encode(), int(norm), float(cdist), int(prefix_start),
+                 int(prefix_length), int(is_short))
+
+
+def segment_host(series, min_segment_length: int, prefix_skip: int = 0):
+    """adaptive_segmentation<T> (segmentation.hpp:340): segment medians per series."""
+    flat, _, lens = pack_host(series)
+    dt = np.dtype(flat.dtype)
+    cap = _native.lib().odba_segment_capacity(lens.ctypes.data_as(ctypes.c_void_p), len(lens),
+                                              int(min_segment_length))
+    out = np.zeros(max(int(cap), 1), dtype=dt)
+    out_lens = np.zeros(len(lens), dtype=np.uint64)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _native.call(f"odba_segment_host_{_SFX[dt]}", vp(flat), vp(lens), len(lens),
+                 int(min_segment_length), int(prefix_skip), vp(out), vp(out_lens))
+    res, pos = [], 0
+    for L in out_lens:
+        res.append(out[pos:pos + int(L)].copy())
+        pos += int(L)
+    return res

@@ -276,4 +276,37 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
                                    path_triples, path_counts, workspace, workspace_bytes, stream);
 }
 
+size_t odba_segment_capacity(const uint64_t *h_lens, int n, int min_segment_length) {
+  if (n < 1 || !h_lens || min_segment_length < 1) return 0;
+  int dw, spb, k_max;
+  segment_params(min_segment_length, &dw, &spb, &k_max);
+  size_t c = 0;
+  for (int i = 0; i < n; ++i) c += size_t((h_lens[i] + spb - 1) / spb) * size_t(k_max);
+  return c;
+}
+
+size_t odba_segment_workspace_bytes(int n) { return n > 0 ? size_t(n) * 8 + 256 : 256; }
+
+int odba_segment_blocks_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                            const uint64_t *h_lens, int n, int min_segment_length, float *medians,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  if (n < 0 || (n > 0 && (!series || !offsets || !lens || !h_lens || !medians || !workspace)) ||
+      min_segment_length < 1)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or minimum segment length below 1");
+  if (int rc = require_sm100()) return rc;
+  return segment_blocks<float>(series, offsets, lens, h_lens, n, min_segment_length, medians,
+                               workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int odba_segment_blocks_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                            const uint64_t *h_lens, int n, int min_segment_length, double *medians,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  if (n < 0 || (n > 0 && (!series || !offsets || !lens || !h_lens || !medians || !workspace)) ||
+      min_segment_length < 1)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or minimum segment length below 1");
+  if (int rc = require_sm100()) return rc;
+  return segment_blocks<double>(series, offsets, lens, h_lens, n, min_segment_length, medians,
+                                workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
 }  // extern "C"

@@ -1,0 +1,1152 @@
+// C++ host side of the drop-in: the reference's templated entry points
+// (include/opendba.hpp) implemented over the C ABI, with the reference's
+// input readers (cpu_utils.hpp), output writers (dba.hpp, io_utils.hpp) and
+// control flow (performDBA, dba.hpp:863-1189; setupAndRun, openDBA.cuh:13-200).
+//
+// Files written, byte-identical to the reference for identical values
+// (std::ostream default formatting, 6 significant digits):
+//   <prefix>.pair_dists.txt             dba.hpp:186-216
+//   <prefix>.avg.txt (append)           dba.hpp:1004-1031, 1126-1131
+//   <prefix>.<c>.path<k>.txt            io_utils.hpp:285-323 (last round of each cluster)
+//   <prefix>.<c>.evolving_centroid.txt  io_utils.hpp:57-76 (every round, removed on convergence)
+//   <prefix>.segmented_seqs.txt         io_utils.hpp:242-261
+// The reference rewrites every path file in every round; only the last
+// round's version survives, so only that one is written here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <limits>
+#include <numeric>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "opendba.hpp"
+#include "opendba_b200.h"
+
+namespace {
+
+[[noreturn]] void die(int code) { std::exit(code); }
+
+void check(int status, const char *what) {
+  if (status != ODBA_OK) {
+    std::cerr << "Device library error in " << what << ": " << odba_status_string(status) << ": "
+              << odba_last_error() << std::endl;
+    die(odba_exit::DEVICE_LIBRARY_ERROR);
+  }
+}
+
+void check_cuda(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    std::cerr << "CUDA error: " << cudaGetErrorString(e) << " (" << what << ")" << std::endl;
+    die(int(e));
+  }
+}
+
+bool file_exists(const std::string &f) {
+  std::ifstream in(f);
+  return in.good();
+}
+
+template <typename T>
+struct Ops;
+template <>
+struct Ops<float> {
+  static int pairwise(const float *s, const uint64_t *o, const uint64_t *l, int n, uint64_t ml,
+                      int os, int oe, float *d, void *w, size_t wb, void *st) {
+    return odba_dtw_pairwise_f32(s, o, l, n, ml, os, oe, d, w, wb, st);
+  }
+  static int znorm(float *s, const uint64_t *o, const uint64_t *l, int n, double *m, double *sg,
+                   void *st) {
+    return odba_znorm_f32(s, o, l, n, m, sg, st);
+  }
+  static int segment(const float *s, const uint64_t *o, const uint64_t *l, const uint64_t *hl,
+                     int n, int minseg, float *med, void *w, size_t wb, void *st) {
+    return odba_segment_blocks_f32(s, o, l, hl, n, minseg, med, w, wb, st);
+  }
+  static int round(const float *c, uint64_t Lc, const float *s, const uint64_t *o,
+                   const uint64_t *l, const uint64_t *hl, int n, int os, int oe, float *mean,
+                   uint32_t *cnt, double *delta, int32_t *tri, int64_t *tc, void *w, size_t wb,
+                   void *st) {
+    return odba_dba_round_f32(c, Lc, s, o, l, hl, n, os, oe, mean, cnt, delta, tri, tc, w, wb, st);
+  }
+};
+template <>
+struct Ops<double> {
+  static int pairwise(const double *s, const uint64_t *o, const uint64_t *l, int n, uint64_t ml,
+                      int os, int oe, double *d, void *w, size_t wb, void *st) {
+    return odba_dtw_pairwise_f64(s, o, l, n, ml, os, oe, d, w, wb, st);
+  }
+  static int znorm(double *s, const uint64_t *o, const uint64_t *l, int n, double *m, double *sg,
+                   void *st) {
+    return odba_znorm_f64(s, o, l, n, m, sg, st);
+  }
+  static int segment(const double *s, const uint64_t *o, const uint64_t *l, const uint64_t *hl,
+                     int n, int minseg, double *med, void *w, size_t wb, void *st) {
+    return odba_segment_blocks_f64(s, o, l, hl, n, minseg, med, w, wb, st);
+  }
+  static int round(const double *c, uint64_t Lc, const double *s, const uint64_t *o,
+                   const uint64_t *l, const uint64_t *hl, int n, int os, int oe, double *mean,
+                   uint32_t *cnt, double *delta, int32_t *tri, int64_t *tc, void *w, size_t wb,
+                   void *st) {
+    return odba_dba_round_f64(c, Lc, s, o, l, hl, n, os, oe, mean, cnt, delta, tri, tc, w, wb, st);
+  }
+};
+
+// RAII device buffer.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  explicit DevBuf(size_t b = 0) { resize(b); }
+  void resize(size_t b) {
+    if (b <= bytes && p) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (b) {
+      check_cuda(cudaMalloc(&p, b), "device allocation in the host façade");
+      bytes = b;
+    }
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+};
+
+template <typename U>
+U *ptr(const DevBuf &b) {
+  return static_cast<U *>(b.p);
+}
+
+// A ragged set of series resident on the device, concatenated.
+template <typename T>
+struct DeviceSet {
+  DevBuf data, offs, lens;
+  std::vector<uint64_t> h_offs, h_lens;
+  int n = 0;
+  uint64_t max_len = 0, total = 0;
+
+  // Copies sequences[i][0..lens[i]) from any memory space.
+  void upload(T *const *sequences, const size_t *lengths, int count, cudaStream_t st) {
+    n = count;
+    h_offs.assign(n, 0);
+    h_lens.assign(n, 0);
+    total = 0;
+    max_len = 0;
+    for (int i = 0; i < n; ++i) {
+      h_offs[i] = total;
+      h_lens[i] = lengths[i];
+      total += lengths[i];
+      max_len = std::max<uint64_t>(max_len, lengths[i]);
+    }
+    data.resize((total + 16) * sizeof(T));
+    offs.resize(std::max(1, n) * sizeof(uint64_t));
+    lens.resize(std::max(1, n) * sizeof(uint64_t));
+    for (int i = 0; i < n; ++i)
+      check_cuda(cudaMemcpyAsync(ptr<T>(data) + h_offs[i], sequences[i], lengths[i] * sizeof(T),
+                                 cudaMemcpyDefault, st),
+                 "series upload");
+    check_cuda(cudaMemcpyAsync(offs.p, h_offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st),
+               "offsets upload");
+    check_cuda(cudaMemcpyAsync(lens.p, h_lens.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st),
+               "lengths upload");
+  }
+};
+
+template <typename T>
+std::vector<T> fetch_series(const T *p, size_t len) {
+  std::vector<T> v(len);
+  if (len) check_cuda(cudaMemcpy(v.data(), p, len * sizeof(T), cudaMemcpyDefault), "series read-back");
+  return v;
+}
+
+// ---- path file (io_utils.hpp:285-323) ----
+const char *move_name(int mv) {
+  switch (mv) {
+    case 1: return "DIAG";
+    case 2: return "RIGHT";
+    case 3: return "UP";
+    case 4: return "OPEN_RIGHT";
+    case 255: return "NIL";
+    case 5: return "NIL_OPEN_RIGHT";
+    default: return "?";
+  }
+}
+
+template <typename T>
+bool write_path_file(const std::string &fname, const char *name, const std::vector<T> &seq,
+                     const std::vector<T> &centroid, bool flip, const int32_t *tri, int64_t count) {
+  std::ofstream path(fname);
+  if (!path.is_open()) {
+    std::cerr << "Cannot write to " << fname << std::endl;
+    return false;
+  }
+  path << name << std::endl;
+  for (int64_t k = 0; k + 1 < count; ++k) {
+    const int i = tri[3 * k], j = tri[3 * k + 1], mv = tri[3 * k + 2];
+    if (flip)
+      path << j << "\t" << seq[j] << "\t" << i << "\t" << centroid[i] << "\t" << move_name(mv)
+           << std::endl;
+    else
+      path << i << "\t" << seq[i] << "\t" << j << "\t" << centroid[j] << "\t" << move_name(mv)
+           << std::endl;
+  }
+  if (count > 0) {
+    const int64_t k = count - 1;
+    const int i = tri[3 * k], j = tri[3 * k + 1], mv = tri[3 * k + 2];
+    path << i << "\t" << seq[i] << "\t" << j << "\t" << centroid[j] << "\t"
+         << (mv == 255 ? "NIL" : (mv == 5 ? "NIL_OPEN_RIGHT" : "?")) << std::endl;
+  }
+  return true;
+}
+
+// ---- checkpoint (io_utils.hpp:57-115) ----
+bool g_warned_checkpoint = false;
+
+template <typename T>
+void write_checkpoint(const std::string &fname, const T *c, size_t len) {
+  std::ofstream f(fname);
+  if (!f.is_open()) {
+    if (!g_warned_checkpoint) {
+      g_warned_checkpoint = true;
+      std::cerr << "Cannot open centroid convergence checkpoint file " << fname
+                << " for writing, no checkpointing for this cluster will be done (i.e. computation "
+                   "cannot be resumed if the program dies unexpectedly)"
+                << std::endl;
+    }
+    return;
+  }
+  f << c[0];
+  for (size_t i = 1; i < len; ++i) f << " " << c[i];
+  f << std::endl;
+}
+
+template <typename T>
+bool read_checkpoint(const std::string &fname, T *c, size_t len) {
+  if (!file_exists(fname)) return false;
+  std::ifstream f(fname);
+  if (!f.is_open()) {
+    std::cerr << "Cannot open existing centroid convergence checkpoint file " << fname
+              << " for reading, will have to restart convergence for this cluster from the start (medoid)"
+              << std::endl;
+    return false;
+  }
+  std::string line;
+  if (!std::getline(f, line)) {
+    std::cerr << "Existing centroid convergence checkpoint file " << fname
+              << "is blank, will have to restart convergence for this cluster from the start (centroid = medoid)"
+              << std::endl;
+    return false;
+  }
+  std::vector<std::string> values;
+  {
+    std::stringstream ss(line);
+    std::string tok;
+    while (std::getline(ss, tok, ' ')) values.push_back(tok);
+  }
+  if (values.size() != len) {
+    std::cerr << "Existing centroid convergence checkpoint file " << fname
+              << " contents does not have the same sequence length as the cluster medoid ("
+              << values.size() << " != " << len
+              << "), assuming corrupt checkpoint file and will have to restart convergence for this "
+                 "cluster from the start (centroid = medoid)"
+              << std::endl;
+    return false;
+  }
+  std::cerr << "Resuming convergence from partially converged centroid in file " << fname << std::endl;
+  std::stringstream ss(line);
+  for (size_t i = 0; i < len; ++i) ss >> c[i];
+  return true;
+}
+
+// ---- membership file (io_utils.hpp:160-240) ----
+int *read_medoid_indices(const std::string &fname, int n, char **names, int *membership) {
+  std::ifstream f(fname);
+  if (!f.is_open()) {
+    std::cerr << "Cannot open sequence cluster membership file " << fname << " for reading" << std::endl;
+    die(odba_exit::CANNOT_READ_MEMBERSHIP);
+  }
+  std::string line;
+  std::getline(f, line);
+  if (line.compare(0, 1, "#")) {
+    std::cerr << "The existing sequence cluster membership file " << fname
+              << " has a first line without the expected '#' comment start" << std::endl;
+    die(odba_exit::MEMBERSHIP_FILE_FORMAT_VIOLATION);
+  }
+  auto split = [](const std::string &s) {
+    std::vector<std::string> out;
+    std::stringstream ss(s);
+    std::string tok;
+    while (std::getline(ss, tok, '\t')) out.push_back(tok);
+    return out;
+  };
+  auto find = [&](const std::string &nm) {
+    for (int i = 0; i < n; ++i)
+      if (nm.compare(names[i]) == 0) return i;
+    return -1;
+  };
+  int max_cluster = 0, line_number = 1;
+  std::vector<std::vector<std::string>> rows;
+  while (std::getline(f, line)) {
+    ++line_number;
+    auto v = split(line);
+    if (v.size() != 3) {
+      std::cerr << "The existing sequence cluster membership file " << fname << " has a line (#"
+                << line_number << ") without the expected three columns (found " << v.size() << ")"
+                << std::endl;
+      die(odba_exit::MEMBERSHIP_FILE_FORMAT_VIOLATION);
+    }
+    int cl = 0;
+    try {
+      cl = std::stoi(v[1]);
+    } catch (const std::exception &ex) {
+      std::cerr << "The existing sequence cluster membership file " << fname << " has a line (#"
+                << line_number << ") where the second tab-delimited column value (" << v[1]
+                << ") is not an integer as expected: " << ex.what() << std::endl;
+      die(odba_exit::MEMBERSHIP_FILE_FORMAT_VIOLATION);
+    }
+    max_cluster = std::max(max_cluster, cl);
+    const int si = find(v[0]);
+    if (si == -1) {
+      std::cerr << "The existing sequence cluster membership file " << fname << " has a line (#"
+                << line_number << ") with a sequence name not found in the input (" << v[0]
+                << " not in existing list of " << n << " names)" << std::endl;
+      die(odba_exit::MEMBERSHIP_FILE_FORMAT_VIOLATION);
+    }
+    membership[si] = cl;
+    rows.push_back(v);
+  }
+  // The reference sizes the medoid array by the largest cluster index it saw
+  // (io_utils.hpp:220); one more slot keeps the last cluster addressable.
+  int *medoids = new int[max_cluster + 1];
+  for (int c = 0; c <= max_cluster; ++c) medoids[c] = -1;
+  for (const auto &v : rows)
+    if (v[0] == v[2]) medoids[std::stoi(v[1])] = find(v[0]);
+  return medoids;
+}
+
+// Medoid pass on device-resident series: distances, pair_dists.txt, medoid
+// (dba.hpp:170-351 for one cluster).
+template <typename T>
+int *medoid_pass(const T *d_data, const uint64_t *d_offs, const uint64_t *d_lens,
+                 const std::vector<uint64_t> &h_lens, int n, uint64_t max_len, char **names, int os,
+                 int oe, const char *output_prefix, double *cdist, int *memberships,
+                 cudaStream_t st) {
+  const size_t npairs = size_t(n) * (n - 1) / 2;
+  std::vector<T> dists(npairs);
+  if (n >= 2) {
+    DevBuf d_dists(npairs * sizeof(T));
+    DevBuf ws(odba_dtw_pairwise_workspace_bytes(sizeof(T), max_len));
+    check(Ops<T>::pairwise(d_data, d_offs, d_lens, n, max_len, os, oe, ptr<T>(d_dists), ws.p,
+                           ws.bytes, st),
+          "all-pairs DTW");
+    check_cuda(cudaMemcpyAsync(dists.data(), d_dists.p, npairs * sizeof(T), cudaMemcpyDeviceToHost, st),
+               "distance download");
+    check_cuda(cudaStreamSynchronize(st), "all-pairs DTW");
+  }
+  std::vector<T> sos(n, T(0));
+  T max_distance = T(0);
+  std::ofstream mats((std::string(output_prefix) + ".pair_dists.txt").c_str());
+  size_t off = 0;
+  for (int s = 0; s + 1 < n; ++s) {
+    mats << names[s];
+    for (int pad = 0; pad < s; ++pad) mats << "\t";
+    mats << "\t0";
+    for (int j = s + 1; j < n; ++j) {
+      T d = dists[off + (j - s - 1)];
+      if (max_distance < d) max_distance = d;
+      mats << "\t" << d;
+      d *= d;
+      sos[s] += d;
+      sos[j] += d;
+    }
+    off += n - s - 1;
+    mats << std::endl;
+  }
+  mats << names[n - 1];
+  for (int pad = 0; pad < n; ++pad) mats << "\t";
+  mats << "0" << std::endl;
+  mats.close();
+  if (*cdist != 1) {
+    std::cerr << "Clustering thresholds other than 1 (complete linkage) are not available in this "
+                 "build; use 1 for a single consensus"
+              << std::endl;
+    die(odba_exit::MEDOID_FINDING_ERROR);
+  }
+  for (int i = 0; i < n; ++i) memberships[i] = 0;
+  std::cerr << "There are 1 clusters" << std::endl;
+  int *medoids = new int[1];
+  int medoid = -1;
+  if (n > 2) {
+    T lowest = std::numeric_limits<T>::max();
+    for (int i = 0; i < n; ++i)
+      if (sos[i] < lowest) {
+        medoid = i;
+        lowest = sos[i];
+      }
+  } else if (n == 2) {
+    medoid = h_lens[0] > h_lens[1] ? 0 : 1;
+  } else {
+    medoid = 0;
+  }
+  if (medoid == -1) {
+    std::cerr << "Logic error in medoid finding routine" << std::endl;
+    die(odba_exit::MEDOID_FINDING_ERROR);
+  }
+  std::cerr << "Processing cluster 0 membership=" << n << ", medoid is " << medoid << std::endl;
+  medoids[0] = medoid;
+  return medoids;
+}
+
+// Runs DBA rounds for one cluster on device-resident members; returns the
+// converged centroid (unscaled) and writes the checkpoint and path files.
+template <typename T>
+std::vector<T> converge_cluster(const DeviceSet<T> &all, const std::vector<int> &member_idx,
+                                char **names, const std::vector<T> &seed, int os, int oe,
+                                const std::string &cluster_prefix, cudaStream_t st) {
+  const int n = int(member_idx.size());
+  const size_t Lc = seed.size();
+  std::vector<uint64_t> m_offs(n), m_lens(n);
+  for (int k = 0; k < n; ++k) {
+    m_offs[k] = all.h_offs[member_idx[k]];
+    m_lens[k] = all.h_lens[member_idx[k]];
+  }
+  DevBuf d_moffs(n * sizeof(uint64_t)), d_mlens(n * sizeof(uint64_t));
+  check_cuda(cudaMemcpyAsync(d_moffs.p, m_offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "member offsets");
+  check_cuda(cudaMemcpyAsync(d_mlens.p, m_lens.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "member lengths");
+  DevBuf ws(odba_dba_round_workspace_bytes(sizeof(T), m_lens.data(), n, Lc, os, oe));
+  DevBuf d_c(Lc * sizeof(T)), d_mean(Lc * sizeof(T)), d_counts(Lc * sizeof(uint32_t)),
+      d_delta(sizeof(double));
+  size_t cap = 0;
+  for (int k = 0; k < n; ++k) cap += m_lens[k] + Lc + 1;
+  DevBuf d_tri(3 * cap * sizeof(int32_t)), d_tc(n * sizeof(int64_t));
+  std::vector<T> centroid = seed, input_centroid = seed, nb(Lc), prev(Lc, T(0)), two_prev(Lc, T(0));
+  check_cuda(cudaMemcpyAsync(d_c.p, centroid.data(), Lc * sizeof(T), cudaMemcpyHostToDevice, st), "centroid upload");
+  const int max_rounds = 250;
+  const std::string ckpt = cluster_prefix + ".evolving_centroid.txt";
+  for (int i = 0; i < max_rounds; ++i) {
+    input_centroid = centroid;
+    check(Ops<T>::round(ptr<T>(d_c), Lc, ptr<T>(all.data), ptr<uint64_t>(d_moffs),
+                        ptr<uint64_t>(d_mlens), m_lens.data(), n, os, oe, ptr<T>(d_mean),
+                        ptr<uint32_t>(d_counts), ptr<double>(d_delta), ptr<int32_t>(d_tri),
+                        ptr<int64_t>(d_tc), ws.p, ws.bytes, st),
+          "DBA round");
+    double delta = 0;
+    check_cuda(cudaMemcpyAsync(nb.data(), d_mean.p, Lc * sizeof(T), cudaMemcpyDeviceToHost, st), "centroid download");
+    check_cuda(cudaMemcpyAsync(&delta, d_delta.p, sizeof(double), cudaMemcpyDeviceToHost, st), "delta download");
+    check_cuda(cudaStreamSynchronize(st), "DBA round");
+    std::cerr << "New delta is " << delta << std::endl;
+    if (delta == 0) break;
+    if (os || oe) {
+      // two_prev starts zeroed (fresh page-locked memory in the reference, dba.hpp:1053-1056)
+      if (i >= 1 && !std::memcmp(nb.data(), two_prev.data(), sizeof(T) * Lc)) {
+        std::cerr << "Detected a flip-flop between two alternative converged centroids (should "
+                     "happen only in open end mode), keeping the first one calculated"
+                  << std::endl;
+        break;
+      }
+      if (i > 1) two_prev = prev;
+      if (i > 0) prev = nb;
+    }
+    write_checkpoint(ckpt, nb.data(), Lc);
+    centroid = nb;
+    check_cuda(cudaMemcpyAsync(d_c.p, centroid.data(), Lc * sizeof(T), cudaMemcpyHostToDevice, st), "centroid upload");
+  }
+  // path files of the last round (each member against that round's input centroid)
+  std::vector<int64_t> tc(n);
+  std::vector<int32_t> tri(3 * cap);
+  check_cuda(cudaMemcpy(tc.data(), d_tc.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost), "path counts");
+  check_cuda(cudaMemcpy(tri.data(), d_tri.p, 3 * cap * sizeof(int32_t), cudaMemcpyDeviceToHost), "paths");
+  std::vector<size_t> tri_off(n);
+  size_t acc = 0;
+  for (int k = 0; k < n; ++k) {
+    tri_off[k] = acc;
+    acc += m_lens[k] + Lc + 1;
+  }
+  const unsigned nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned w = 0; w < nthreads; ++w) {
+    pool.emplace_back([&, w]() {
+      for (int k = int(w); k < n; k += int(nthreads)) {
+        std::vector<T> seq(m_lens[k]);
+        cudaMemcpy(seq.data(), ptr<T>(all.data) + m_offs[k], m_lens[k] * sizeof(T), cudaMemcpyDeviceToHost);
+        const bool flip = oe && Lc < m_lens[k];
+        write_path_file<T>(cluster_prefix + ".path" + std::to_string(k) + ".txt",
+                           names[member_idx[k]], seq, input_centroid, flip,
+                           tri.data() + 3 * tri_off[k], tc[k]);
+      }
+    });
+  }
+  for (auto &t : pool) t.join();
+  return nb;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+
+template <typename T>
+void normalizeSequences(T **sequences, size_t num_sequences, size_t *sequence_lengths,
+                        int refSequenceIndex, double *sequence_means, double *sequence_sigmas,
+                        cudaStream_t stream) {
+  if (refSequenceIndex >= 0 && size_t(refSequenceIndex) < num_sequences) {
+    std::cerr << "Rescaling to a reference sequence's mean and deviation is not available; "
+                 "only z-normalisation (refSequenceIndex < 0)"
+              << std::endl;
+    die(odba_exit::DEVICE_LIBRARY_ERROR);
+  }
+  DeviceSet<T> ds;
+  ds.upload(sequences, sequence_lengths, int(num_sequences), stream);
+  DevBuf m(num_sequences * sizeof(double) + 8), s(num_sequences * sizeof(double) + 8);
+  check(Ops<T>::znorm(ptr<T>(ds.data), ptr<uint64_t>(ds.offs), ptr<uint64_t>(ds.lens),
+                      int(num_sequences), ptr<double>(m), ptr<double>(s), stream),
+        "z-normalisation");
+  for (size_t i = 0; i < num_sequences; ++i)
+    check_cuda(cudaMemcpyAsync(sequences[i], ptr<T>(ds.data) + ds.h_offs[i],
+                               sequence_lengths[i] * sizeof(T), cudaMemcpyDefault, stream),
+               "normalised series write-back");
+  if (sequence_means)
+    check_cuda(cudaMemcpyAsync(sequence_means, m.p, num_sequences * sizeof(double), cudaMemcpyDefault, stream), "means");
+  if (sequence_sigmas)
+    check_cuda(cudaMemcpyAsync(sequence_sigmas, s.p, num_sequences * sizeof(double), cudaMemcpyDefault, stream), "sigmas");
+  check_cuda(cudaStreamSynchronize(stream), "z-normalisation");
+}
+
+template <typename T>
+int *approximateMedoidIndices(T *gpu_sequences, size_t maxSeqLength, size_t num_sequences,
+                              size_t *sequence_lengths, char **sequence_names, int use_open_start,
+                              int use_open_end, char *output_prefix, double *cdist,
+                              int *memberships, cudaStream_t stream) {
+  const int n = int(num_sequences);
+  std::vector<T *> ptrs(n);
+  for (int i = 0; i < n; ++i) ptrs[i] = gpu_sequences + size_t(i) * maxSeqLength;
+  DeviceSet<T> ds;
+  ds.upload(ptrs.data(), sequence_lengths, n, stream);
+  return medoid_pass<T>(ptr<T>(ds.data), ptr<uint64_t>(ds.offs), ptr<uint64_t>(ds.lens), ds.h_lens,
+                        n, ds.max_len, sequence_names, use_open_start, use_open_end, output_prefix,
+                        cdist, memberships, stream);
+}
+
+template <typename T>
+double DBAUpdate(T *C, size_t centerLength, T **sequences, char **sequence_names,
+                 size_t num_sequences, size_t *sequence_lengths, int use_open_start,
+                 int use_open_end, T *updatedMean, std::string output_prefix, cudaStream_t stream) {
+  const int n = int(num_sequences);
+  DeviceSet<T> ds;
+  ds.upload(sequences, sequence_lengths, n, stream);
+  std::vector<T> centroid = fetch_series(C, centerLength);
+  DevBuf ws(odba_dba_round_workspace_bytes(sizeof(T), ds.h_lens.data(), n, centerLength,
+                                           use_open_start, use_open_end));
+  DevBuf d_c(centerLength * sizeof(T)), d_mean(centerLength * sizeof(T)),
+      d_counts(centerLength * sizeof(uint32_t)), d_delta(sizeof(double));
+  size_t cap = 0;
+  for (int k = 0; k < n; ++k) cap += ds.h_lens[k] + centerLength + 1;
+  DevBuf d_tri(3 * cap * sizeof(int32_t)), d_tc(n * sizeof(int64_t));
+  check_cuda(cudaMemcpyAsync(d_c.p, centroid.data(), centerLength * sizeof(T), cudaMemcpyHostToDevice, stream), "centroid upload");
+  check(Ops<T>::round(ptr<T>(d_c), centerLength, ptr<T>(ds.data), ptr<uint64_t>(ds.offs),
+                      ptr<uint64_t>(ds.lens), ds.h_lens.data(), n, use_open_start, use_open_end,
+                      ptr<T>(d_mean), ptr<uint32_t>(d_counts), ptr<double>(d_delta),
+                      ptr<int32_t>(d_tri), ptr<int64_t>(d_tc), ws.p, ws.bytes, stream),
+        "DBA round");
+  double delta = 0;
+  check_cuda(cudaMemcpyAsync(updatedMean, d_mean.p, centerLength * sizeof(T), cudaMemcpyDefault, stream), "centroid download");
+  check_cuda(cudaMemcpyAsync(&delta, d_delta.p, sizeof(double), cudaMemcpyDeviceToHost, stream), "delta download");
+  check_cuda(cudaStreamSynchronize(stream), "DBA round");
+  if (!output_prefix.empty()) {
+    std::vector<int64_t> tc(n);
+    std::vector<int32_t> tri(3 * cap);
+    check_cuda(cudaMemcpy(tc.data(), d_tc.p, n * sizeof(int64_t), cudaMemcpyDeviceToHost), "path counts");
+    check_cuda(cudaMemcpy(tri.data(), d_tri.p, 3 * cap * sizeof(int32_t), cudaMemcpyDeviceToHost), "paths");
+    size_t off = 0;
+    for (int k = 0; k < n; ++k) {
+      std::vector<T> seq = fetch_series(ptr<T>(ds.data) + ds.h_offs[k], ds.h_lens[k]);
+      const bool flip = use_open_end && centerLength < ds.h_lens[k];
+      if (!write_path_file<T>(output_prefix + ".path" + std::to_string(k) + ".txt",
+                              sequence_names[k], seq, centroid, flip, tri.data() + 3 * off, tc[k]))
+        return odba_exit::CANNOT_WRITE_DTW_PATH_MATRIX;
+      off += ds.h_lens[k] + centerLength + 1;
+    }
+  }
+  return delta;
+}
+
+template <typename T>
+void performDBA(T **sequences, int num_sequences, size_t *sequence_lengths, char **sequence_names,
+                int use_open_start, int use_open_end, char *output_prefix, int norm_sequences,
+                double cdist, char **series_file_names, int num_series, int read_mode,
+                bool is_segmented, int algo_mode, cudaStream_t stream) {
+  (void)series_file_names;
+  (void)num_series;
+  (void)read_mode;
+  (void)is_segmented;
+  const int n = num_sequences;
+  // sanitise the last sample (dba.hpp:868-872)
+  for (int i = 0; i < n; ++i) {
+    if (sequence_lengths[i] == 0) continue;
+    T last;
+    check_cuda(cudaMemcpy(&last, sequences[i] + sequence_lengths[i] - 1, sizeof(T), cudaMemcpyDefault),
+               "reading a last sample");
+    if (last >= std::sqrt(std::numeric_limits<T>::max())) sequence_lengths[i]--;
+  }
+  // stable sort by length; pointers, names and lengths permuted in place (dba.hpp:876-885)
+  {
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return sequence_lengths[a] < sequence_lengths[b]; });
+    std::vector<T *> s2(n);
+    std::vector<char *> n2(n);
+    std::vector<size_t> l2(n);
+    for (int i = 0; i < n; ++i) {
+      s2[i] = sequences[order[i]];
+      n2[i] = sequence_names[order[i]];
+      l2[i] = sequence_lengths[order[i]];
+    }
+    for (int i = 0; i < n; ++i) {
+      sequences[i] = s2[i];
+      sequence_names[i] = n2[i];
+      sequence_lengths[i] = l2[i];
+    }
+  }
+  DeviceSet<T> ds;
+  ds.upload(sequences, sequence_lengths, n, stream);
+  std::vector<double> means(n, 0.0), sigmas(n, 1.0);
+  if (norm_sequences) {
+    DevBuf m(n * sizeof(double) + 8), s(n * sizeof(double) + 8);
+    check(Ops<T>::znorm(ptr<T>(ds.data), ptr<uint64_t>(ds.offs), ptr<uint64_t>(ds.lens), n,
+                        ptr<double>(m), ptr<double>(s), stream),
+          "z-normalisation");
+    check_cuda(cudaMemcpyAsync(means.data(), m.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream), "means");
+    check_cuda(cudaMemcpyAsync(sigmas.data(), s.p, n * sizeof(double), cudaMemcpyDeviceToHost, stream), "sigmas");
+    // the reference normalises the caller's series in place
+    for (int i = 0; i < n; ++i)
+      check_cuda(cudaMemcpyAsync(sequences[i], ptr<T>(ds.data) + ds.h_offs[i],
+                                 sequence_lengths[i] * sizeof(T), cudaMemcpyDefault, stream),
+                 "normalised series write-back");
+    check_cuda(cudaStreamSynchronize(stream), "z-normalisation");
+  }
+  std::vector<int> membership(n, 0);
+  int *medoids = nullptr;
+  if (algo_mode == CLUSTER_AND_CONSENSUS || algo_mode == CLUSTER_ONLY) {
+    medoids = medoid_pass<T>(ptr<T>(ds.data), ptr<uint64_t>(ds.offs), ptr<uint64_t>(ds.lens),
+                             ds.h_lens, n, ds.max_len, sequence_names, use_open_start,
+                             use_open_end, output_prefix, &cdist, membership.data(), stream);
+  } else if (algo_mode == CONSENSUS_ONLY) {
+    std::cerr << "Reading previous clustering data" << std::endl;
+    medoids = read_medoid_indices(std::string(output_prefix) + ".cluster_membership.txt", n,
+                                  sequence_names, membership.data());
+  } else {
+    std::cerr << "Call to performDBA included an unrecognized algorithm mode " << algo_mode
+              << " (programming error, please contact the developer)" << std::endl;
+    die(odba_exit::UNKNOWN_ALGO);
+  }
+  int num_clusters = 1;
+  for (int i = 0; i < n; ++i) num_clusters = std::max(num_clusters, membership[i] + 1);
+  if (cdist != 1 && algo_mode != CONSENSUS_ONLY) {
+    const std::string mf = std::string(output_prefix) + ".cluster_membership.txt";
+    std::ofstream membership_file(mf.c_str());
+    if (!membership_file.is_open()) {
+      std::cerr << "Cannot open sequence cluster membership file " << mf << " for writing" << std::endl;
+      die(odba_exit::CANNOT_WRITE_MEMBERSHIP);
+    }
+    membership_file << "## cluster distance threshold was " << cdist << std::endl;
+    for (int i = 0; i < n; ++i)
+      membership_file << sequence_names[i] << "\t" << membership[i] << "\t"
+                      << sequence_names[medoids[membership[i]]] << std::endl;
+  }
+  if (algo_mode == CLUSTER_ONLY) {
+    delete[] medoids;
+    return;
+  }
+  const std::string avg_name = std::string(output_prefix) + ".avg.txt";
+  int curr = 0;
+  if (file_exists(avg_name)) {
+    // text-mode builds of the reference count no finished averages and always
+    // resume at cluster index 1 (io_utils.hpp:119-123, dba.hpp:982-986)
+    curr = 1;
+    std::cerr << "Restarting convergence with cluster " << (curr + 1) << "/" << num_clusters
+              << " based on checkpoint in " << avg_name << std::endl;
+  }
+  std::ofstream avgs(avg_name.c_str(), std::ios::app);
+  if (!avgs.is_open()) {
+    std::cerr << "Cannot open sequence averages file " << output_prefix << ".avg.txt for writing" << std::endl;
+    die(odba_exit::CANNOT_WRITE_DBA_AVG);
+  }
+  for (; curr < num_clusters; ++curr) {
+    std::vector<int> members;
+    for (int i = 0; i < n; ++i)
+      if (membership[i] == curr) members.push_back(i);
+    const int med = medoids[curr];
+    const size_t medoid_len = sequence_lengths[med];
+    std::vector<T> medoid_seq = fetch_series(ptr<T>(ds.data) + ds.h_offs[med], medoid_len);
+    if (members.size() == 1) {
+      std::cerr << "Outputting singleton sequence " << sequence_names[med] << " as-is (a.k.a. cluster "
+                << (curr + 1) << "/" << num_clusters << ")." << std::endl;
+      avgs << sequence_names[med];
+      for (size_t i = 0; i < medoid_len; ++i) {
+        if (norm_sequences)
+          avgs << "\t" << ((T)(means[med] + medoid_seq[i] * sigmas[med]));
+        else
+          avgs << "\t" << medoid_seq[i];
+      }
+      avgs << std::endl;
+      avgs.flush();
+      continue;
+    }
+    const std::string cprefix = std::string(output_prefix) + "." + std::to_string(curr);
+    std::vector<T> seed = medoid_seq;
+    read_checkpoint(cprefix + ".evolving_centroid.txt", seed.data(), medoid_len);
+    std::cerr << "Processing cluster " << (curr + 1) << " of " << num_clusters << ", "
+              << members.size() << " members, medoid " << sequence_names[med] << " has length "
+              << medoid_len << std::endl;
+    std::vector<T> nb = converge_cluster<T>(ds, members, sequence_names, seed, use_open_start,
+                                            use_open_end, cprefix, stream);
+    if (norm_sequences)
+      for (size_t i = 0; i < medoid_len; ++i) nb[i] = (T)(means[med] + nb[i] * sigmas[med]);
+    avgs << sequence_names[med];
+    for (size_t i = 0; i < medoid_len; ++i) avgs << "\t" << nb[i];
+    avgs << std::endl;
+    avgs.flush();
+    const std::string ck = cprefix + ".evolving_centroid.txt";
+    if (std::remove(ck.c_str()) != 0)
+      std::cerr << "Warning: could not remove temporary checkpoint file " << ck << std::endl;
+  }
+  delete[] medoids;
+}
+
+// Block-edge merge and sentinel removal after the segmentation kernel
+// (segmentation.hpp:486-578).  segmented_sequences / segmented_seq_lengths are
+// allocated with cudaMallocManaged, as the reference does, for the caller to free.
+template <typename T>
+void adaptive_segmentation(T **sequences, size_t *seq_lengths, int num_seqs, int min_segment_length,
+                           T ***segmented_sequences, size_t **segmented_seq_lengths,
+                           int prefix_length_to_skip, cudaStream_t stream) {
+  const int n = num_seqs;
+  DeviceSet<T> ds;
+  ds.upload(sequences, seq_lengths, n, stream);
+  const size_t cap = odba_segment_capacity(ds.h_lens.data(), n, min_segment_length);
+  DevBuf d_med(std::max<size_t>(cap, 1) * sizeof(T));
+  DevBuf ws(odba_segment_workspace_bytes(n));
+  check(Ops<T>::segment(ptr<T>(ds.data), ptr<uint64_t>(ds.offs), ptr<uint64_t>(ds.lens),
+                        ds.h_lens.data(), n, min_segment_length, ptr<T>(d_med), ws.p, ws.bytes,
+                        stream),
+        "segmentation");
+  std::vector<T> med(cap);
+  check_cuda(cudaMemcpyAsync(med.data(), d_med.p, cap * sizeof(T), cudaMemcpyDeviceToHost, stream), "segment download");
+  check_cuda(cudaStreamSynchronize(stream), "segmentation");
+  check_cuda(cudaMallocManaged(segmented_sequences, sizeof(T *) * std::max(1, n)), "segmented sequence pointers");
+  check_cuda(cudaMallocManaged(segmented_seq_lengths, sizeof(size_t) * std::max(1, n)), "segmented lengths");
+  int dw = (min_segment_length + 2) / 3;
+  const int spb = 256 * dw;
+  const float per = float(min_segment_length) / float(dw);
+  const int k_max = int((256 + per - 1) / per);
+  const T TMAX = std::numeric_limits<T>::max();
+  size_t base = 0;
+  for (int i = 0; i < n; ++i) {
+    T *seg = med.data() + base;
+    const size_t slen = size_t(k_max) * size_t((ds.h_lens[i] + spb - 1) / spb);
+    base += slen;
+    T epsilon = TMAX;
+    T previous = seg[0];
+    for (size_t j = 1; j < slen; ++j) {
+      const T current = seg[j];
+      if (current != TMAX && previous != TMAX &&
+          ((current <= previous && previous - current < epsilon) ||
+           (current > previous && current - previous < epsilon))) {
+        if (current - previous == 0) {
+          for (size_t k = j; k < slen; k++) {
+            seg[k - 1] = seg[k];
+            if (seg[k] == TMAX) break;
+          }
+        } else {
+          epsilon = current < previous ? (previous - current) : (current - previous);
+        }
+      }
+      previous = current;
+    }
+    bool prev_undef = false;
+    long cursor = 0;
+    for (size_t j = 0; j < slen; ++j) {
+      if (seg[j] == TMAX) {
+        prev_undef = true;
+        continue;
+      }
+      if (prev_undef) {
+        prev_undef = false;
+        if (cursor >= 1 && seg[cursor - 1] < seg[j] + epsilon && seg[cursor - 1] > seg[j] - epsilon)
+          seg[cursor - 1] = (seg[cursor - 1] + seg[j]) / 2;
+      }
+      if (size_t(cursor) != j) seg[cursor] = seg[j];
+      cursor++;
+    }
+    if (cursor >= 1 && seg[cursor - 1] >= TMAX / 2) cursor--;
+    long skipped = 0;
+    if (prefix_length_to_skip) {
+      if (cursor <= prefix_length_to_skip) {
+        skipped = cursor - 1;
+        cursor = 1;
+      } else {
+        skipped = prefix_length_to_skip;
+        cursor -= prefix_length_to_skip;
+      }
+    }
+    (*segmented_seq_lengths)[i] = size_t(cursor);
+    check_cuda(cudaMallocManaged(&(*segmented_sequences)[i], sizeof(T) * std::max<long>(cursor, 1)),
+               "a segmented sequence");
+    std::memcpy((*segmented_sequences)[i], seg + skipped, sizeof(T) * size_t(cursor));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Readers (cpu_utils.hpp:60-134, 381-456, 553-624).
+
+namespace {
+
+template <typename T>
+int read_text_data(const char *fname, std::vector<T> &out) {
+  std::ifstream ifs(fname);
+  if (!ifs) {
+    std::cerr << "Error reading in file " << fname << ", skipping" << std::endl;
+    return 1;
+  }
+  size_t lines = 0;
+  {
+    std::vector<char> buf(1 << 20);
+    while (true) {
+      ifs.read(buf.data(), buf.size());
+      const std::streamsize got = ifs.gcount();
+      if (got <= 0) break;
+      lines += size_t(std::count(buf.begin(), buf.begin() + got, '\n'));
+    }
+  }
+  if (lines == 0) {
+    std::cerr << "File " << fname << " is empty or not properly formatted. Skipping." << std::endl;
+    return 1;
+  }
+  out.assign(lines, T(0));
+  ifs.clear();
+  ifs.seekg(0, std::ios::beg);
+  std::stringstream in;
+  std::string line;
+  for (size_t i = 0; i < lines; ++i) {
+    std::getline(ifs, line);
+    in.str(line);
+    in >> out[i];
+    in.clear();
+  }
+  return 0;
+}
+
+template <typename T>
+int read_binary_data(const char *fname, std::vector<T> &out, bool is_short) {
+  std::ifstream ifs(fname, std::ios::binary);
+  if (!ifs) return 1;
+  ifs.seekg(0, ifs.end);
+  const std::streamoff bytes = ifs.tellg();
+  ifs.seekg(0, std::ios::beg);
+  if (is_short) {
+    std::vector<short> raw(size_t(bytes) / 2);
+    ifs.read(reinterpret_cast<char *>(raw.data()), raw.size() * 2);
+    out.resize(raw.size());
+    for (size_t i = 0; i < raw.size(); ++i) out[i] = T(float(raw[i]));
+  } else {
+    out.resize(size_t(bytes) / sizeof(T));
+    ifs.read(reinterpret_cast<char *>(out.data()), out.size() * sizeof(T));
+  }
+  return 0;
+}
+
+template <typename T>
+int read_tsv_data(const char *fname, std::vector<std::vector<T>> &seqs,
+                  std::vector<std::string> &names) {
+  std::ifstream ifs(fname);
+  if (!ifs) return 0;
+  int count = 0;
+  for (std::string line; std::getline(ifs, line);) {
+    const size_t cols = size_t(std::count(line.begin(), line.end(), '\t'));
+    std::vector<T> s(cols, T(0));
+    std::istringstream iss(line);
+    std::string name;
+    iss >> name;
+    size_t k = 0;
+    while (iss.good()) {
+      T v = T(0);
+      iss >> v;
+      if (k < cols) s[k] = v;
+      ++k;
+    }
+    seqs.push_back(std::move(s));
+    names.push_back(name);
+    ++count;
+  }
+  return count;
+}
+
+char *dup_cstr(const std::string &s) {
+  char *p = new char[s.size() + 1];
+  std::memcpy(p, s.c_str(), s.size() + 1);
+  return p;
+}
+
+template <typename T>
+int write_sequences(T **seqs, size_t *lens, char **names, int n, const std::string &fname) {
+  std::ofstream out(fname);
+  if (!out.is_open()) {
+    std::cerr << "Cannot write to " << fname << std::endl;
+    return odba_exit::CANNOT_WRITE_DTW_PATH_MATRIX;
+  }
+  for (int i = 0; i < n; ++i) {
+    std::vector<T> s = fetch_series(seqs[i], lens[i]);
+    out << names[i] << "\t" << s[0];
+    for (size_t j = 1; j < lens[i]; ++j) out << "\t" << s[j];
+    out << std::endl;
+  }
+  return 0;
+}
+
+}  // namespace
+
+template <typename T>
+void setupAndRun(char *seqprefix_file_name, char **series_file_names, int num_series,
+                 char *output_prefix, int read_mode, int use_open_start, int use_open_end,
+                 char *min_segment_length_string, int norm_sequences, double cdist,
+                 const int prefix_start, const int prefix_length, bool is_short) {
+  int min_segment_length_2 = -1;
+  char *pos = std::strchr(min_segment_length_string, ',');
+  if (pos) {
+    min_segment_length_2 = std::atoi(pos + 1);
+    *pos = '\0';
+  }
+  const int min_segment_length = std::atoi(min_segment_length_string);
+
+  std::vector<std::vector<T>> data;
+  std::vector<std::string> names;
+  if (read_mode == TSV_READ_MODE) {
+    std::cerr << "Step 1 of 3: Loading " << num_series << (num_series == 1 ? " TSV data file" : " TSV data files") << std::endl;
+    for (int i = 0; i < num_series; ++i)
+      if (read_tsv_data<T>(series_file_names[i], data, names) < 1)
+        std::cerr << "Error reading in TSV file " << series_file_names[i] << ", skipping" << std::endl;
+  } else {
+    const bool binary = read_mode == BINARY_READ_MODE;
+    std::cerr << "Step 1 of 3: Loading " << num_series
+              << (binary ? (num_series == 1 ? " binary data file" : " binary data files")
+                         : (num_series == 1 ? " text data file" : " text data files"))
+              << ", total sequence count " << num_series << std::endl;
+    for (int i = 0; i < num_series; ++i) {
+      std::vector<T> s;
+      const int rc = binary ? read_binary_data<T>(series_file_names[i], s, is_short)
+                            : read_text_data<T>(series_file_names[i], s);
+      if (rc) {
+        std::cerr << "Error reading in " << (binary ? "binary" : "text") << " file "
+                  << series_file_names[i] << ", skipping" << std::endl;
+        continue;
+      }
+      data.push_back(std::move(s));
+      names.push_back(series_file_names[i]);
+    }
+  }
+  int n = int(data.size());
+  if (n < 2) {
+    std::cerr << "At least two sequences must be provided to calculate an average, but found " << n
+              << ", aborting" << std::endl;
+    die(odba_exit::NOT_ENOUGH_SEQUENCES);
+  }
+  // shorten names to everything before the first "." (openDBA.cuh:58-59)
+  for (auto &nm : names) {
+    const size_t dot = nm.find('.');
+    if (dot != std::string::npos) nm.resize(dot);
+  }
+  if (seqprefix_file_name != nullptr) {
+    std::cerr << "Prefix chopping (a leader sequence) is not available in this build" << std::endl;
+    die(odba_exit::CANNOT_READ_SEQUENCE_PREFIX_FILE);
+  }
+  std::vector<T *> seq_ptrs(n);
+  std::vector<size_t> lens(n);
+  std::vector<char *> name_ptrs(n);
+  for (int i = 0; i < n; ++i) {
+    seq_ptrs[i] = data[i].data();
+    lens[i] = data[i].size();
+    name_ptrs[i] = dup_cstr(names[i]);
+  }
+  T **segs = nullptr;
+  size_t *seglens = nullptr;
+  if (min_segment_length > 0) {
+    adaptive_segmentation<T>(seq_ptrs.data(), lens.data(), n, min_segment_length, &segs, &seglens,
+                             prefix_start);
+    int removed = 0;
+    for (int i = 0; i < n; ++i) {
+      const int j = i - removed;
+      if (seglens[j] < 2 || (prefix_length > 0 && seglens[j] < size_t(prefix_length))) {
+        cudaFree(segs[j]);
+        for (int k = j + 1; k < n - removed; ++k) {
+          segs[k - 1] = segs[k];
+          seglens[k - 1] = seglens[k];
+          name_ptrs[k - 1] = name_ptrs[k];
+        }
+        ++removed;
+      }
+    }
+    if (removed) {
+      std::cerr << "Removing " << removed << " segmented sequences that are too short, as they may "
+                << "unduly skew the convergence process. To retain more sequences, consider setting "
+                << "a smaller minimum segment size (currently " << min_segment_length << ")" << std::endl;
+      n -= removed;
+      if (n < 2) {
+        std::cerr << "At least two sequences must survive segmentation filters to calculate an "
+                     "average, but found " << n << ", aborting" << std::endl;
+        die(odba_exit::NOT_ENOUGH_SEQUENCES);
+      }
+    }
+    if (prefix_length > 0)
+      for (int i = 0; i < n; ++i) seglens[i] = size_t(prefix_length);
+    write_sequences<T>(segs, seglens, name_ptrs.data(), n,
+                       std::string(output_prefix) + ".segmented_seqs.txt");
+    if (min_segment_length_2 != -1) {
+      std::cerr << "Performing cluster generation with segment size of " << min_segment_length << std::endl;
+      performDBA<T>(segs, n, seglens, name_ptrs.data(), use_open_start, use_open_end, output_prefix,
+                    norm_sequences, cdist, series_file_names, num_series, read_mode,
+                    min_segment_length > 1, CLUSTER_ONLY);
+    } else {
+      for (int i = 0; i < n; ++i) {
+        seq_ptrs[i] = segs[i];
+        lens[i] = seglens[i];
+      }
+    }
+  }
+  if (min_segment_length_2 != -1) {
+    std::cerr << "Performing consensus generation with segment size of " << min_segment_length_2 << std::endl;
+    performDBA<T>(seq_ptrs.data(), n, lens.data(), name_ptrs.data(), use_open_start, use_open_end,
+                  output_prefix, norm_sequences, cdist, series_file_names, num_series, read_mode,
+                  min_segment_length > 1, CONSENSUS_ONLY);
+  } else {
+    std::cerr << "Performing both clustering and consensus generation with segment size of "
+              << min_segment_length << std::endl;
+    performDBA<T>(seq_ptrs.data(), n, lens.data(), name_ptrs.data(), use_open_start, use_open_end,
+                  output_prefix, norm_sequences, cdist, series_file_names, num_series, read_mode,
+                  min_segment_length > 1, CLUSTER_AND_CONSENSUS);
+  }
+  if (segs) {
+    for (int i = 0; i < n; ++i) cudaFree(segs[i]);
+    cudaFree(segs);
+    cudaFree(seglens);
+  }
+  for (auto p : name_ptrs) delete[] p;
+}
+
+#define ODBA_INSTANTIATE(T)                                                                     \
+  template void setupAndRun<T>(char *, char **, int, char *, int, int, int, char *, int, double, \
+                               const int, const int, bool);                                     \
+  template void performDBA<T>(T **, int, size_t *, char **, int, int, char *, int, double,       \
+                              char **, int, int, bool, int, cudaStream_t);                       \
+  template int *approximateMedoidIndices<T>(T *, size_t, size_t, size_t *, char **, int, int,    \
+                                            char *, double *, int *, cudaStream_t);              \
+  template double DBAUpdate<T>(T *, size_t, T **, char **, size_t, size_t *, int, int, T *,      \
+                               std::string, cudaStream_t);                                       \
+  template void normalizeSequences<T>(T **, size_t, size_t *, int, double *, double *,           \
+                                      cudaStream_t);                                            \
+  template void adaptive_segmentation<T>(T **, size_t *, int, int, T ***, size_t **, int,        \
+                                         cudaStream_t);
+ODBA_INSTANTIATE(float)
+ODBA_INSTANTIATE(double)
+
+// ---------------------------------------------------------------------------
+// C entry points over the façade (declared in opendba_b200.h).  Like the
+// reference's host code they end the process with its exit codes on fatal
+// errors (missing files, unwritable outputs, too few sequences).
+
+extern "C" int odba_perform_dba_f32(float **sequences, int num_sequences, size_t *lengths,
+                                    char **names, int use_open_start, int use_open_end,
+                                    const char *output_prefix, int norm, double cdist,
+                                    int algo_mode) {
+  std::string pfx(output_prefix ? output_prefix : "");
+  std::vector<char> buf(pfx.begin(), pfx.end());
+  buf.push_back('\0');
+  performDBA<float>(sequences, num_sequences, lengths, names, use_open_start, use_open_end,
+                    buf.data(), norm, cdist, nullptr, 0, BINARY_READ_MODE, false, algo_mode);
+  return ODBA_OK;
+}
+
+extern "C" int odba_perform_dba_f64(double **sequences, int num_sequences, size_t *lengths,
+                                    char **names, int use_open_start, int use_open_end,
+                                    const char *output_prefix, int norm, double cdist,
+                                    int algo_mode) {
+  std::string pfx(output_prefix ? output_prefix : "");
+  std::vector<char> buf(pfx.begin(), pfx.end());
+  buf.push_back('\0');
+  performDBA<double>(sequences, num_sequences, lengths, names, use_open_start, use_open_end,
+                     buf.data(), norm, cdist, nullptr, 0, BINARY_READ_MODE, false, algo_mode);
+  return ODBA_OK;
+}
+
+extern "C" int odba_setup_and_run(int elem_size, const char *seqprefix_file, char **files,
+                                  int num_files, const char *output_prefix, int read_mode,
+                                  int use_open_start, int use_open_end,
+                                  const char *min_segment_length, int norm, double cdist,
+                                  int prefix_start, int prefix_length, int is_short) {
+  std::vector<char> pfx(output_prefix, output_prefix + std::strlen(output_prefix) + 1);
+  std::vector<char> ms(min_segment_length, min_segment_length + std::strlen(min_segment_length) + 1);
+  std::vector<char> leader;
+  if (seqprefix_file) leader.assign(seqprefix_file, seqprefix_file + std::strlen(seqprefix_file) + 1);
+  char *lp = seqprefix_file ? leader.data() : nullptr;
+  if (elem_size == 8)
+    setupAndRun<double>(lp, files, num_files, pfx.data(), read_mode, use_open_start, use_open_end,
+                        ms.data(), norm, cdist, prefix_start, prefix_length, is_short != 0);
+  else
+    setupAndRun<float>(lp, files, num_files, pfx.data(), read_mode, use_open_start, use_open_end,
+                       ms.data(), norm, cdist, prefix_start, prefix_length, is_short != 0);
+  return ODBA_OK;
+}
+
+namespace {
+template <typename T>
+int segment_host(const T *h_series, const uint64_t *h_lens, int n, int minseg, int prefix_skip,
+                 T *h_out, uint64_t *h_out_lens) {
+  std::vector<T *> ptrs(n);
+  std::vector<size_t> lens(n);
+  size_t off = 0;
+  for (int i = 0; i < n; ++i) {
+    ptrs[i] = const_cast<T *>(h_series + off);
+    lens[i] = h_lens[i];
+    off += h_lens[i];
+  }
+  T **segs = nullptr;
+  size_t *seglens = nullptr;
+  adaptive_segmentation<T>(ptrs.data(), lens.data(), n, minseg, &segs, &seglens, prefix_skip);
+  size_t pos = 0;
+  for (int i = 0; i < n; ++i) {
+    std::memcpy(h_out + pos, segs[i], seglens[i] * sizeof(T));
+    pos += seglens[i];
+    h_out_lens[i] = seglens[i];
+    cudaFree(segs[i]);
+  }
+  cudaFree(segs);
+  cudaFree(seglens);
+  return ODBA_OK;
+}
+}  // namespace
+
+extern "C" int odba_segment_host_f32(const float *h_series, const uint64_t *h_lens, int n,
+                                     int min_segment_length, int prefix_skip, float *h_out,
+                                     uint64_t *h_out_lens) {
+  if (n < 1 || !h_series || !h_lens || !h_out || !h_out_lens || min_segment_length < 1)
+    return ODBA_ERR_INVALID_ARGUMENT;
+  return segment_host<float>(h_series, h_lens, n, min_segment_length, prefix_skip, h_out, h_out_lens);
+}
+
+extern "C" int odba_segment_host_f64(const double *h_series, const uint64_t *h_lens, int n,
+                                     int min_segment_length, int prefix_skip, double *h_out,
+                                     uint64_t *h_out_lens) {
+  if (n < 1 || !h_series || !h_lens || !h_out || !h_out_lens || min_segment_length < 1)
+    return ODBA_ERR_INVALID_ARGUMENT;
+  return segment_host<double>(h_series, h_lens, n, min_segment_length, prefix_skip, h_out, h_out_lens);
+}

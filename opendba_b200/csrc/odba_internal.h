@@ -42,4 +42,10 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
                      uint32_t *counts, double *delta, int32_t *triples, int64_t *triple_counts,
                      void *ws, size_t ws_bytes, cudaStream_t stream);
 
+void segment_params(int minseg, int *dw, int *spb, int *k_max);
+template <typename T>
+int segment_blocks(const T *series, const uint64_t *offsets, const uint64_t *lens,
+                   const uint64_t *h_lens, int n, int minseg, T *medians, void *ws,
+                   size_t ws_bytes, cudaStream_t stream);
+
 }  // namespace odba

@@ -21,6 +21,7 @@
 #include <math.h>
 #include <omp.h>
 #include <stdlib.h>
+#include <limits.h>
 #include <string.h>
 
 /* The reference's swath width: blockDim.x of every DTWDistance launch
@@ -478,3 +479,282 @@ DEFINE_ZNORM(double, f64)
 
 DEFINE_FAST(float, f32, fmaf, fminf, FLT_MAX)
 DEFINE_FAST(double, f64, fma, fmin, DBL_MAX)
+
+/* ---- k-segmentation (segmentation.hpp:48-337 kernel, 340-583 host) ---------
+ * One "block" = raw_samples_per_threadblock = 256 * dw samples of one series,
+ * processed as the reference's 256-thread block does, thread by thread.
+ * Where the reference races (the even-span median of a 2-sample segment
+ * reads the first sample of the next segment while that segment is being
+ * sorted), the sorted value is used.  smem is the device's opt-in shared
+ * memory per block; it sets the DP extent e. */
+static unsigned char seg_quant(double v) {
+  /* float -> unsigned char conversion on the GPU clamps to [0, 255], NaN -> 0 */
+  if (!(v == v)) return 0;
+  if (v <= 0.0) return 0;
+  if (v >= 255.0) return 255;
+  return (unsigned char)v;
+}
+
+#define DEFINE_SEG(T, SFX, TMAX, TMIN)                                                         \
+  static void seg_block_##SFX(const T *series, long orig_N, int by, int spb, int k_max,      \
+                              int minseg, int smem, T *out_medians) {                        \
+    const int dw = (minseg + 2) / 3;                                                         \
+    const int N = ((long)(by + 1) * spb > orig_N) ? (int)(orig_N % spb) : spb;              \
+    int expected_k = k_max;                                                                  \
+    if ((long)(by + 1) * spb > orig_N) {                                                     \
+      int per = (spb + k_max - 1) / k_max;                                                   \
+      expected_k = ((int)(orig_N % spb) + per - 1) / per;                                     \
+    }                                                                                        \
+    const int N_ds = N / dw;                                                                 \
+    const T *x = series + (long)by * spb;                                                    \
+    T ds[256];                                                                               \
+    for (int t = 0; t < 256; ++t) ds[t] = 0;                                                 \
+    for (int t = 0; t < 256; ++t) {                                                          \
+      if (t * dw <= N - dw) {                                                                \
+        T acc = 0;                                                                           \
+        int num = 0;                                                                         \
+        for (int i = 0; i < dw && dw * t + t + i < N; i++) {                                 \
+          acc = acc + x[dw * t + i];                                                         \
+          num++;                                                                             \
+        }                                                                                    \
+        ds[t] = acc / (T)num;                                                                \
+      }                                                                                      \
+    }                                                                                        \
+    /* warp shuffle-down reductions with "if (tmp < val) val = tmp" (cuda_utils.hpp:20-40) */ \
+    T wmax[8], wmin[8];                                                                      \
+    for (int w = 0; w < 8; ++w) {                                                            \
+      T vmax[32], vmin[32];                                                                  \
+      for (int l = 0; l < 32; ++l) {                                                         \
+        int t = w * 32 + l;                                                                  \
+        vmax[l] = t < N_ds ? ds[t] : TMIN;                                                   \
+        vmin[l] = t < N_ds ? ds[t] : TMAX;                                                   \
+      }                                                                                      \
+      for (int off = 16; off > 0; off /= 2) {                                                \
+        T nmax[32], nmin[32];                                                                \
+        for (int l = 0; l < 32; ++l) {                                                       \
+          T a = l + off < 32 ? vmin[l + off] : vmin[l];                                      \
+          T b = l + off < 32 ? vmax[l + off] : vmax[l];                                      \
+          nmin[l] = (a < vmin[l]) ? a : vmin[l];                                             \
+          nmax[l] = (b > vmax[l]) ? b : vmax[l];                                             \
+        }                                                                                    \
+        memcpy(vmin, nmin, sizeof(vmin));                                                    \
+        memcpy(vmax, nmax, sizeof(vmax));                                                    \
+      }                                                                                      \
+      wmax[w] = vmax[0];                                                                     \
+      wmin[w] = vmin[0];                                                                     \
+    }                                                                                        \
+    const int nw = N_ds / 32;                                                                \
+    T gmax, gmin;                                                                            \
+    {                                                                                        \
+      T vmax[32], vmin[32];                                                                  \
+      for (int l = 0; l < 32; ++l) {                                                         \
+        vmax[l] = l < nw ? wmax[l] : TMIN;                                                   \
+        vmin[l] = l < nw ? wmin[l] : TMAX;                                                   \
+      }                                                                                      \
+      for (int off = 16; off > 0; off /= 2) {                                                \
+        T nmax[32], nmin[32];                                                                \
+        for (int l = 0; l < 32; ++l) {                                                       \
+          T a = l + off < 32 ? vmin[l + off] : vmin[l];                                      \
+          T b = l + off < 32 ? vmax[l + off] : vmax[l];                                      \
+          nmin[l] = (a < vmin[l]) ? a : vmin[l];                                             \
+          nmax[l] = (b > vmax[l]) ? b : vmax[l];                                             \
+        }                                                                                    \
+        memcpy(vmin, nmin, sizeof(vmin));                                                    \
+        memcpy(vmax, nmax, sizeof(vmax));                                                    \
+      }                                                                                      \
+      gmax = vmax[0];                                                                        \
+      gmin = vmin[0];                                                                        \
+    }                                                                                        \
+    /* only thread 0 repoints T_min at the block minimum (segmentation.hpp:144-148); the    \
+     * others read slot N_ds/32 of the max array: warp 0's minimum, or with fewer than two  \
+     * full warps the value thread 0 wrote there */                                          \
+    T others_min = nw >= 2 ? wmin[0] : (nw == 1 ? gmin : gmax);                             \
+    unsigned char q[256];                                                                    \
+    for (int t = 0; t < N_ds; ++t) {                                                         \
+      T mn = t == 0 ? gmin : others_min;                                                     \
+      T frac = (ds[t] - mn) / (gmax - mn + 1);                                               \
+      q[t] = seg_quant(256.0 * (double)frac);                                                \
+    }                                                                                        \
+    /* prefix sums give every SUMS / SQUARES entry (no 16-bit wrap for <= 256 samples) */   \
+    unsigned P[257], Q[257];                                                                 \
+    P[0] = Q[0] = 0;                                                                         \
+    for (int t = 0; t < N_ds; ++t) {                                                         \
+      P[t + 1] = P[t] + q[t];                                                                \
+      Q[t + 1] = Q[t] + (unsigned)q[t] * q[t];                                               \
+    }                                                                                        \
+    /* DP extent from the reference's shared-memory layout (segmentation.hpp:96-162) */     \
+    int e = 1;                                                                               \
+    if (N_ds > 0) {                                                                          \
+      long off_opt = ((long)(k_max + 1) * 2 + 3) / 4 * 4;                                    \
+      long off_ksd = off_opt + (long)(N_ds + 1) * 4;                                         \
+      long off_ds = (off_ksd + 2L * (N_ds + 1) * 4 + sizeof(T) - 1) / sizeof(T) * sizeof(T); \
+      long off_sq = (off_ds + (long)(N_ds + 2) * sizeof(T) + 3) / 4 * 4;                     \
+      e = (int)((smem - off_sq) / ((long)N_ds * 6));                                         \
+    }                                                                                        \
+    /* 1-based DIST(l, r): SQUARES - SUMS*SUMS/len, unsigned minus int (int product wraps) */ \
+    unsigned *ksd0 = (unsigned *)calloc(N_ds + 2, sizeof(unsigned));                         \
+    unsigned *ksd1 = (unsigned *)calloc(N_ds + 2, sizeof(unsigned));                         \
+    unsigned short *kpath = (unsigned short *)calloc((size_t)(k_max + 1) * (N_ds + 2), 2);  \
+    unsigned short bp[260];                                                                  \
+    int smallest_noisy = expected_k + 1;                                                     \
+    int test_k = (expected_k + 1) / 2;                                                       \
+    int delta = test_k / 2;                                                                  \
+    int exitf = 0;                                                                           \
+    while (!exitf) {                                                                         \
+      for (int t = 0; t < N_ds; ++t) {                                                       \
+        int n1 = t + 1;                                                                      \
+        if (n1 <= e) {                                                                       \
+          unsigned s = P[n1] - P[0];                                                         \
+          unsigned sq = Q[n1] - Q[0];                                                        \
+          int ms = (int)((unsigned)(s * s)) / n1;                                            \
+          ksd1[n1] = sq - (unsigned)ms;                                                      \
+        } else {                                                                             \
+          ksd1[n1] = INT_MAX / 2;                                                            \
+        }                                                                                    \
+        if (t < test_k) kpath[(size_t)t * (N_ds + 2) + t] = (unsigned short)(test_k - 1);    \
+      }                                                                                      \
+      for (int p = 2; p <= test_k; ++p) {                                                    \
+        unsigned *prev = (p % 2) ? ksd0 : ksd1;                                              \
+        unsigned *cur = (p % 2) ? ksd1 : ksd0;                                               \
+        for (int n = p; n <= N_ds; ++n) {                                                    \
+          int lo = (n - e + 1 > p) ? n - e + 1 : p;                                          \
+          int minval = INT_MAX, minidx = -1;                                                 \
+          for (int idx = lo, start = lo; idx - start < e && idx <= n; idx++) {               \
+            unsigned s = P[n] - P[idx - 1];                                                  \
+            unsigned sq = Q[n] - Q[idx - 1];                                                 \
+            int len = n - idx + 1;                                                           \
+            int ms = (int)((unsigned)(s * s)) / len;                                         \
+            unsigned opt = prev[idx - 1] + (sq - (unsigned)ms);                              \
+            if (opt < (unsigned)minval) {                                                    \
+              minval = (int)opt;                                                             \
+              minidx = idx;                                                                  \
+            }                                                                                \
+          }                                                                                  \
+          cur[n] = (unsigned)minval;                                                         \
+          kpath[(size_t)(p - 1) * (N_ds + 2) + (n - 1)] = (unsigned short)((unsigned short)minidx - 1); \
+        }                                                                                    \
+      }                                                                                      \
+      bp[test_k] = (unsigned short)N_ds;                                                     \
+      for (int p = test_k - 1; p >= 1; p--) {                                                \
+        int col = bp[p + 1] - 1;                                                             \
+        bp[p] = (col >= 0 && col < N_ds + 2) ? kpath[(size_t)p * (N_ds + 2) + col] : 0;      \
+      }                                                                                      \
+      bp[0] = 0;                                                                             \
+      int noisy = 0;                                                                         \
+      for (int i = 1; i <= test_k; i++)                                                      \
+        if ((int)bp[i] - (int)bp[i - 1] < minseg / dw) noisy = 1;                            \
+      if (delta == 0 || test_k + delta > k_max) {                                            \
+        exitf = 1;                                                                           \
+      } else if (test_k != 1 && noisy) {                                                     \
+        smallest_noisy = test_k;                                                             \
+        test_k -= delta;                                                                     \
+      } else {                                                                               \
+        if (test_k == 1 || smallest_noisy == test_k + 1)                                     \
+          exitf = 1;                                                                         \
+        else                                                                                 \
+          test_k += delta;                                                                   \
+      }                                                                                      \
+      delta = (delta + 1) / 2;                                                               \
+    }                                                                                        \
+    /* medians: segments sorted, then the reference's quirky middle pick */                 \
+    T *od = (T *)calloc((size_t)spb + 2, sizeof(T));                                         \
+    for (int i = 0; i < spb && (long)by * spb + i < orig_N; ++i) od[i] = x[i];               \
+    for (int t = test_k + 1; t <= k_max; ++t) out_medians[t - 1] = TMAX;                     \
+    for (int t = 1; t <= test_k; ++t) {                                                      \
+      int rb = bp[t] * dw;                                                                   \
+      if (rb > N) rb = N;                                                                    \
+      int lb = bp[t - 1] * dw;                                                               \
+      for (int i = lb; i < rb - 1; ++i)                                                      \
+        for (int j = i + 1; j < rb; ++j)                                                     \
+          if (od[i] > od[j]) {                                                               \
+            T tmp = od[i];                                                                   \
+            od[i] = od[j];                                                                   \
+            od[j] = tmp;                                                                     \
+          }                                                                                  \
+    }                                                                                        \
+    for (int t = 1; t <= test_k; ++t) {                                                      \
+      int rb = bp[t] * dw;                                                                   \
+      if (rb > N) rb = N;                                                                    \
+      int lb = bp[t - 1] * dw;                                                               \
+      if ((lb - rb) % 2)                                                                     \
+        out_medians[t - 1] = od[(lb + rb) / 2];                                              \
+      else                                                                                   \
+        out_medians[t - 1] = (od[(lb + rb) / 2] + od[(lb + rb) / 2 + 1]) / 2;                \
+    }                                                                                        \
+    free(ksd0);                                                                              \
+    free(ksd1);                                                                              \
+    free(kpath);                                                                             \
+    free(od);                                                                                \
+  }                                                                                          \
+                                                                                             \
+  int64_t oracle_segment_##SFX(const T *series, const uint64_t *offsets, const uint64_t *lens,  \
+                               int n, int minseg, int prefix_skip, int smem, T *out,          \
+                               uint64_t *out_lens) {                                          \
+    const int dw = (minseg + 2) / 3;                                                         \
+    const int spb = 256 * dw;                                                                \
+    const int k_max = (int)((256 + ((float)minseg) / dw - 1) / (((float)minseg) / dw));      \
+    int64_t written = 0;                                                                     \
+    for (int s = 0; s < n; ++s) {                                                            \
+      const long L = (long)lens[s];                                                          \
+      const int nb = (int)((L + spb - 1) / spb);                                             \
+      size_t cap = (size_t)k_max * nb;                                                       \
+      T *seg = (T *)malloc(sizeof(T) * (cap ? cap : 1));                                     \
+      for (int by = 0; by < nb; ++by)                                                        \
+        seg_block_##SFX(series + offsets[s], L, by, spb, k_max, minseg, smem,               \
+                        seg + (size_t)by * k_max);                                           \
+      /* host post-processing (segmentation.hpp:492-573) */                                  \
+      T epsilon = TMAX;                                                                      \
+      T previous = seg[0];                                                                   \
+      for (size_t j = 1; j < cap; ++j) {                                                     \
+        T current = seg[j];                                                                  \
+        if (current != TMAX && previous != TMAX &&                                           \
+            ((current <= previous && previous - current < epsilon) ||                        \
+             (current > previous && current - previous < epsilon))) {                        \
+          if (current - previous == 0) {                                                     \
+            for (size_t k = j; k < cap; k++) {                                               \
+              seg[k - 1] = seg[k];                                                           \
+              if (seg[k] == TMAX) break;                                                     \
+            }                                                                                \
+          } else {                                                                           \
+            epsilon = current < previous ? (previous - current) : (current - previous);      \
+          }                                                                                  \
+        }                                                                                    \
+        previous = current;                                                                  \
+      }                                                                                      \
+      int prev_undef = 0;                                                                    \
+      long cursor = 0;                                                                       \
+      for (size_t j = 0; j < cap; ++j) {                                                     \
+        if (seg[j] == TMAX) {                                                                \
+          prev_undef = 1;                                                                    \
+          continue;                                                                          \
+        }                                                                                    \
+        if (prev_undef) {                                                                    \
+          prev_undef = 0;                                                                    \
+          if (cursor >= 1 && seg[cursor - 1] < seg[j] + epsilon &&                           \
+              seg[cursor - 1] > seg[j] - epsilon)                                            \
+            seg[cursor - 1] = (seg[cursor - 1] + seg[j]) / 2;                                \
+        }                                                                                    \
+        if ((size_t)cursor != j) seg[cursor] = seg[j];                                       \
+        cursor++;                                                                            \
+      }                                                                                      \
+      if (cursor >= 1 && seg[cursor - 1] >= TMAX / 2) cursor--;                              \
+      long skipped = 0;                                                                      \
+      if (prefix_skip) {                                                                     \
+        if (cursor <= prefix_skip) {                                                         \
+          skipped = cursor - 1;                                                              \
+          cursor = 1;                                                                        \
+        } else {                                                                             \
+          skipped = prefix_skip;                                                             \
+          cursor -= prefix_skip;                                                             \
+        }                                                                                    \
+      }                                                                                      \
+      out_lens[s] = (uint64_t)cursor;                                                        \
+      memcpy(out + written, seg + skipped, sizeof(T) * (size_t)cursor);                      \
+      written += cursor;                                                                     \
+      free(seg);                                                                             \
+    }                                                                                        \
+    return written;                                                                          \
+  }
+
+DEFINE_SEG(float, f32, FLT_MAX, FLT_MIN)
+DEFINE_SEG(double, f64, DBL_MAX, DBL_MIN)

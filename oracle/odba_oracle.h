@@ -96,6 +96,17 @@ int oracle_znorm_f32(float *series, const uint64_t *offsets, const uint64_t *len
 int oracle_znorm_f64(double *series, const uint64_t *offsets, const uint64_t *lens, int n,
                      double *means, double *sigmas);
 
+/* k-segmentation of every series (adaptive_segmentation, segmentation.hpp:340-583)
+ * with the device's opt-in shared memory per block smem; out receives the
+ * concatenated segment medians, out_lens the segment counts.  Returns the
+ * number of values written. */
+int64_t oracle_segment_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                           int n, int minseg, int prefix_skip, int smem, float *out,
+                           uint64_t *out_lens);
+int64_t oracle_segment_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                           int n, int minseg, int prefix_skip, int smem, double *out,
+                           uint64_t *out_lens);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,9 @@ def lib():
             f.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                           ctypes.c_int, P, ctypes.c_int64]
             f.restype = ctypes.c_int64
+            f = getattr(_lib, f"oracle_segment_{sfx}")
+            f.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P]
+            f.restype = ctypes.c_int64
             f = getattr(_lib, f"oracle_znorm_{sfx}")
             f.argtypes = [P, P, P, ctypes.c_int, P, P]
             f.restype = ctypes.c_int
@@ -167,6 +170,29 @@ def znorm(series):
                                                         _ptr(means), _ptr(sigmas))
     out = [flat[int(o):int(o) + int(L)].copy() for o, L in zip(offsets, lens)]
     return out, means, sigmas
+
+
+B200_SMEM_OPTIN = 232448  # cudaDevAttrMaxSharedMemoryPerBlockOptin on B200
+
+
+def segment(series, minseg, prefix_skip=0, smem=B200_SMEM_OPTIN):
+    """k-segmentation medians per series (adaptive_segmentation)."""
+    flat, offsets, lens = pack(series)
+    n = len(series)
+    dw = (minseg + 2) // 3
+    spb = 256 * dw
+    k_max = int((256 + minseg / dw - 1) / (minseg / dw))
+    cap = sum(k_max * ((int(L) + spb - 1) // spb) for L in lens) + 1
+    out = np.zeros(cap, dtype=flat.dtype)
+    out_lens = np.zeros(n, dtype=np.uint64)
+    getattr(lib(), f"oracle_segment_{_sfx(flat.dtype)}")(
+        _ptr(flat), _ptr(offsets), _ptr(lens), n, minseg, prefix_skip, smem, _ptr(out),
+        _ptr(out_lens))
+    res, pos = [], 0
+    for L in out_lens:
+        res.append(out[pos:pos + int(L)].copy())
+        pos += int(L)
+    return res
 
 
 # ---- series bundle I/O (layout in oracle/series_bundle.h) ----
