@@ -60,6 +60,28 @@ int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const u
                           int n, uint64_t max_len, int use_open_start, int use_open_end,
                           double *dists, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- DTW distances of an arbitrary pair list (batched jobs, queries) ----------
+ * No single reference counterpart: the batched form of the medoid launches of
+ * approximateMedoidIndices (dba.hpp:67-161) over many independent jobs, and
+ * read-vs-centroid queries, in one persistent launch.  Task i aligns series
+ * `first` (rows) against series `second` (columns) of the shared series table
+ * and writes the reference's pair distance (dtw.hpp:116-125, 242-257) to
+ * dists[out & (2^62 - 1)]; bit 62 of `out` selects open start, bit 63 open end.
+ * Tasks are taken in array order (put the largest m*n first).  The workspace
+ * is odba_dtw_pairwise_workspace_bytes(elem_size, max_len) with max_len the
+ * longest `first` series. */
+typedef struct odba_pair_task {
+  uint32_t first;
+  uint32_t second;
+  uint64_t out;
+} odba_pair_task;
+int odba_dtw_pairlist_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                          const odba_pair_task *tasks, uint64_t ntasks, uint64_t max_len,
+                          float *dists, void *workspace, size_t workspace_bytes, void *stream);
+int odba_dtw_pairlist_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                          const odba_pair_task *tasks, uint64_t ntasks, uint64_t max_len,
+                          double *dists, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- all-vs-all DTW distances without any device allocation -----------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory at the call site (a serving or real-time loop that forbids allocation
@@ -123,6 +145,48 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
                        int64_t *path_counts, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* ---- one DBA round for many jobs at once ---------------------------------------
+ * No single reference counterpart: DBAUpdate<T> (dba.hpp:432-848) for many
+ * independent averaging jobs in one launch sequence (no host synchronization
+ * inside, so it can be captured in a CUDA graph and replayed every round).
+ * Job J: centroid centroids[centroid_offsets[J] .. + centroid_lens[J]),
+ * job_flags[J] bit 0 open start, bit 1 open end, bit 2 active (inactive jobs
+ * are skipped and keep their outputs), members job_member_begin[J] ..
+ * job_member_end[J]-1 of the member list, in the order their samples are
+ * added (the reference's member order).  Member k is series member_series[k]
+ * of the series table and belongs to job member_job[k].  member_order
+ * (optional) is the order in which members are aligned (longest first keeps
+ * the tail short); it does not change any result.  Outputs per job at the
+ * job's centroid offset: means, counts; deltas[J] = max |centroid - mean|.
+ * The h_* arrays are host copies that size the workspace.  Results equal one
+ * odba_dba_round_* call per job, bit for bit. */
+size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_lens,
+                                      const int *h_member_job, int nmem,
+                                      const uint64_t *h_centroid_lens, const int *h_job_flags,
+                                      int njobs);
+int odba_dba_batch_round_f32(const float *centroids, const uint64_t *centroid_offsets,
+                             const int *centroid_lens, const int *job_flags,
+                             const int *job_member_begin, const int *job_member_end, int njobs,
+                             int max_centroid_len, const float *series, const uint64_t *offsets,
+                             const uint64_t *lens, const int *member_series,
+                             const int *member_job, const int *member_order, int nmem,
+                             const uint64_t *h_member_lens, const int *h_member_job,
+                             const uint64_t *h_centroid_lens, const int *h_job_flags,
+                             float *means, uint32_t *counts, double *deltas, int32_t *path_triples,
+                             int64_t *path_counts, void *workspace, size_t workspace_bytes,
+                             void *stream);
+int odba_dba_batch_round_f64(const double *centroids, const uint64_t *centroid_offsets,
+                             const int *centroid_lens, const int *job_flags,
+                             const int *job_member_begin, const int *job_member_end, int njobs,
+                             int max_centroid_len, const double *series, const uint64_t *offsets,
+                             const uint64_t *lens, const int *member_series,
+                             const int *member_job, const int *member_order, int nmem,
+                             const uint64_t *h_member_lens, const int *h_member_job,
+                             const uint64_t *h_centroid_lens, const int *h_job_flags,
+                             double *means, uint32_t *counts, double *deltas,
+                             int32_t *path_triples, int64_t *path_counts, void *workspace,
+                             size_t workspace_bytes, void *stream);
+
 /* ---- k-segmentation ------------------------------------------------------------
  * Replaces the kernel part of adaptive_segmentation<T> (adaptive_device_segmentation,
  * segmentation.hpp:48-337; launch segmentation.hpp:440-463).  Every block of
@@ -185,6 +249,27 @@ int odba_segment_host_f32(const float *h_series, const uint64_t *h_lens, int n,
 int odba_segment_host_f64(const double *h_series, const uint64_t *h_lens, int n,
                           int min_segment_length, int prefix_skip, double *h_out,
                           uint64_t *h_out_lens);
+
+/* ---- many DBA jobs: batched or plain ---------------------------------------------
+ * No single reference counterpart: each job is what performDBA<T> computes for
+ * one cluster (cdist 1, CLUSTER_AND_CONSENSUS, no files; dba.hpp:863-1146) for
+ * the series job_begin[j] .. job_end[j]-1 of the concatenated host input (jobs
+ * contiguous and in order), with job_flags[j] bit 0 open start, bit 1 open end.
+ * batched != 0: all pairs of all jobs in one length-sorted launch, and each DBA
+ * round for every unconverged job as one CUDA-graph replay; batched == 0: job
+ * by job through the single-job entry points (the drop-in path).  Both give the
+ * same results.  Outputs per job: h_medoids[j] (index within the job's input
+ * order), its centroid at h_centroids[h_centroid_offsets[j]] with the medoid's
+ * length (capacity: the sum over jobs of the longest series), rounds run and
+ * the last delta.  max_rounds <= 0 means the reference's 250. */
+int odba_dba_jobs_f32(const float *h_series, const uint64_t *h_lens, const int *job_begin,
+                      const int *job_end, const int *job_flags, int njobs, int norm,
+                      int max_rounds, int batched, int *h_medoids, uint64_t *h_centroid_offsets,
+                      float *h_centroids, int *h_rounds, double *h_deltas, void *stream);
+int odba_dba_jobs_f64(const double *h_series, const uint64_t *h_lens, const int *job_begin,
+                      const int *job_end, const int *job_flags, int njobs, int norm,
+                      int max_rounds, int batched, int *h_medoids, uint64_t *h_centroid_offsets,
+                      double *h_centroids, int *h_rounds, double *h_deltas, void *stream);
 
 #ifdef __cplusplus
 }

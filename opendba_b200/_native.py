@@ -33,6 +33,8 @@ SIGNATURES = {
     "odba_dtw_pairwise_workspace_bytes": (ctypes.c_size_t, [I32, U64]),
     "odba_dtw_pairwise_f32": (I32, [P, P, P, I32, U64, I32, I32, P, P, ctypes.c_size_t, P]),
     "odba_dtw_pairwise_f64": (I32, [P, P, P, I32, U64, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_dtw_pairlist_f32": (I32, [P, P, P, P, U64, U64, P, P, ctypes.c_size_t, P]),
+    "odba_dtw_pairlist_f64": (I32, [P, P, P, P, U64, U64, P, P, ctypes.c_size_t, P]),
     "odba_dtw_pairwise_noalloc_f32": (I32, [P, P, P, I32, U64, I32, I32, P, P]),
     "odba_medoid_f32": (I32, [P, P, I32, P, P, P]),
     "odba_medoid_f64": (I32, [P, P, I32, P, P, P]),
@@ -43,6 +45,11 @@ SIGNATURES = {
                                  ctypes.c_size_t, P]),
     "odba_dba_round_f64": (I32, [P, U64, P, P, P, P, I32, I32, I32, P, P, P, P, P, P,
                                  ctypes.c_size_t, P]),
+    "odba_dba_batch_workspace_bytes": (ctypes.c_size_t, [I32, P, P, I32, P, P, I32]),
+    "odba_dba_batch_round_f32": (I32, [P, P, P, P, P, P, I32, I32, P, P, P, P, P, P, I32, P, P, P, P,
+                                       P, P, P, P, P, P, ctypes.c_size_t, P]),
+    "odba_dba_batch_round_f64": (I32, [P, P, P, P, P, P, I32, I32, P, P, P, P, P, P, I32, P, P, P, P,
+                                       P, P, P, P, P, P, ctypes.c_size_t, P]),
     "odba_segment_capacity": (ctypes.c_size_t, [P, I32, I32]),
     "odba_segment_workspace_bytes": (ctypes.c_size_t, [I32]),
     "odba_segment_blocks_f32": (I32, [P, P, P, P, I32, I32, P, P, ctypes.c_size_t, P]),
@@ -55,6 +62,8 @@ SIGNATURES = {
                                  ctypes.c_char_p, I32, ctypes.c_double, I32, I32, I32]),
     "odba_segment_host_f32": (I32, [P, P, I32, I32, I32, P, P]),
     "odba_segment_host_f64": (I32, [P, P, I32, I32, I32, P, P]),
+    "odba_dba_jobs_f32": (I32, [P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P]),
+    "odba_dba_jobs_f64": (I32, [P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P]),
     "odba_medoid_pass_host_f32": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
     "odba_medoid_pass_host_f64": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
 }

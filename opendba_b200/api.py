@@ -236,3 +236,47 @@ def segment_host(series, min_segment_length: int, prefix_skip: int = 0):
         res.append(out[pos:pos + int(L)].copy())
         pos += int(L)
     return res
+
+
+def dba_jobs(jobs, flags=None, norm: int = 1, batched: bool = True, max_rounds: int = 250,
+             dtype=None):
+    """Many independent DBA jobs (odba_dba_jobs_*): each job a list of series.
+
+    flags[j]: bit 0 open start, bit 1 open end.  Returns a list of dicts with
+    the medoid (index within the job), centroid, rounds and last delta."""
+    dtype = np.dtype(dtype or np.asarray(jobs[0][0]).dtype)
+    flat_list, lens, jb, je = [], [], [], []
+    for job in jobs:
+        jb.append(len(lens))
+        for s in job:
+            a = np.ascontiguousarray(s, dtype=dtype)
+            flat_list.append(a)
+            lens.append(len(a))
+        je.append(len(lens))
+    flat = np.ascontiguousarray(np.concatenate(flat_list))
+    lens = np.array(lens, dtype=np.uint64)
+    jb = np.array(jb, dtype=np.int32)
+    je = np.array(je, dtype=np.int32)
+    fl = np.array(flags if flags is not None else [0] * len(jobs), dtype=np.int32)
+    nj = len(jobs)
+    cap = int(sum(max(len(s) for s in job) for job in jobs))
+    med = np.zeros(nj, dtype=np.int32)
+    coff = np.zeros(nj, dtype=np.uint64)
+    cent = np.zeros(max(cap, 1), dtype=dtype)
+    rounds = np.zeros(nj, dtype=np.int32)
+    deltas = np.zeros(nj, dtype=np.float64)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _native.call(f"odba_dba_jobs_{_SFX[dtype]}", vp(flat), vp(lens), vp(jb), vp(je), vp(fl), nj,
+                 int(norm), int(max_rounds), int(bool(batched)), vp(med), vp(coff), vp(cent),
+                 vp(rounds), vp(deltas), None)
+    out = []
+    for j, job in enumerate(jobs):
+        L = len(job[int(med[j])])
+        # truncation of a too-large last sample shortens the medoid by one
+        o = int(coff[j])
+        nxt = int(coff[j + 1]) if j + 1 < nj else None
+        if nxt is not None:
+            L = nxt - o
+        out.append({"medoid": int(med[j]), "centroid": cent[o:o + L].copy(), "rounds": int(rounds[j]),
+                    "delta": float(deltas[j])})
+    return out

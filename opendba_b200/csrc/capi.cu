@@ -247,6 +247,28 @@ int odba_medoid_pass_host_f64(const double *h_series, const uint64_t *h_lens, in
                                   h_medoid, h_means, h_sigmas, stream);
 }
 
+int odba_dtw_pairlist_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                          const odba_pair_task *tasks, uint64_t ntasks, uint64_t max_len,
+                          float *dists, void *workspace, size_t workspace_bytes, void *stream) {
+  if (ntasks && (!series || !offsets || !lens || !tasks || !dists || !workspace))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer");
+  if (max_len == 0 || max_len > (1ull << 31)) return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be in [1, 2^31]");
+  if (int rc = require_sm100()) return rc;
+  return pairlist_launch<float>(series, offsets, lens, tasks, ntasks, max_len, dists, workspace,
+                                workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int odba_dtw_pairlist_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                          const odba_pair_task *tasks, uint64_t ntasks, uint64_t max_len,
+                          double *dists, void *workspace, size_t workspace_bytes, void *stream) {
+  if (ntasks && (!series || !offsets || !lens || !tasks || !dists || !workspace))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer");
+  if (max_len == 0 || max_len > (1ull << 31)) return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be in [1, 2^31]");
+  if (int rc = require_sm100()) return rc;
+  return pairlist_launch<double>(series, offsets, lens, tasks, ntasks, max_len, dists, workspace,
+                                 workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
 size_t odba_dba_round_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
                                       uint64_t centroid_len, int use_open_start, int use_open_end) {
   if (n < 1 || !h_lens || centroid_len == 0) return 0;
@@ -275,6 +297,52 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
                                    use_open_start, use_open_end, new_centroid, counts, delta,
                                    path_triples, path_counts, workspace, workspace_bytes, stream);
 }
+
+size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_lens,
+                                      const int *h_member_job, int nmem,
+                                      const uint64_t *h_centroid_lens, const int *h_job_flags,
+                                      int njobs) {
+  if (nmem < 1 || njobs < 1 || !h_member_lens || !h_member_job || !h_centroid_lens || !h_job_flags)
+    return 0;
+  if (elem_size == 8)
+    return dba_batch_workspace_bytes<double>(h_member_lens, h_member_job, nmem, h_centroid_lens,
+                                             h_job_flags, njobs);
+  return dba_batch_workspace_bytes<float>(h_member_lens, h_member_job, nmem, h_centroid_lens,
+                                          h_job_flags, njobs);
+}
+
+#define ODBA_BATCH_ROUND(SFX, T)                                                               \
+  int odba_dba_batch_round_##SFX(                                                              \
+      const T *centroids, const uint64_t *centroid_offsets, const int *centroid_lens,          \
+      const int *job_flags, const int *job_member_begin, const int *job_member_end, int njobs, \
+      int max_centroid_len, const T *series, const uint64_t *offsets, const uint64_t *lens,    \
+      const int *member_series, const int *member_job, const int *member_order, int nmem,      \
+      const uint64_t *h_member_lens, const int *h_member_job, const uint64_t *h_centroid_lens, \
+      const int *h_job_flags, T *means, uint32_t *counts, double *deltas, int32_t *path_triples, \
+      int64_t *path_counts, void *workspace, size_t workspace_bytes, void *stream) {           \
+    if (njobs < 1 || nmem < 1 || max_centroid_len < 1 || !centroids || !centroid_offsets ||    \
+        !centroid_lens || !job_flags || !job_member_begin || !job_member_end || !series ||     \
+        !offsets || !lens || !member_series || !member_job || !h_member_lens ||                \
+        !h_member_job || !h_centroid_lens || !h_job_flags || !means || !counts || !deltas ||   \
+        !workspace)                                                                            \
+      return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or empty batch");                   \
+    if ((path_triples == nullptr) != (path_counts == nullptr))                                 \
+      return fail(ODBA_ERR_INVALID_ARGUMENT, "path triples and their counts go together");     \
+    for (int k = 0; k < nmem; ++k)                                                             \
+      if (h_member_lens[k] == 0 || h_member_lens[k] > (1ull << 30) || h_member_job[k] < 0 ||   \
+          h_member_job[k] >= njobs)                                                            \
+        return fail(ODBA_ERR_INVALID_ARGUMENT, "bad member length or job index");              \
+    if (int rc = require_sm100()) return rc;                                                   \
+    return dba_batch_launch<T>(                                                                \
+        centroids, reinterpret_cast<const unsigned long long *>(centroid_offsets),             \
+        centroid_lens, job_flags, job_member_begin, job_member_end, njobs, max_centroid_len,   \
+        series, offsets, lens, member_series, member_job, member_order, nmem, h_member_lens,    \
+        h_member_job, h_centroid_lens, h_job_flags, means, counts, deltas, path_triples,        \
+        path_counts, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));           \
+  }
+ODBA_BATCH_ROUND(f32, float)
+ODBA_BATCH_ROUND(f64, double)
+#undef ODBA_BATCH_ROUND
 
 size_t odba_segment_capacity(const uint64_t *h_lens, int n, int min_segment_length) {
   if (n < 1 || !h_lens || min_segment_length < 1) return 0;

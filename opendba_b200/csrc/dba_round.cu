@@ -67,40 +67,63 @@ __host__ __device__ inline MemberGeom member_geom(uint64_t len, uint64_t Lc, int
   return g;
 }
 
+// Jobs share one launch: job J owns centroid centroids[coff[J] .. + clen[J]),
+// flags (bit 0 open start, bit 1 open end, bit 2 active) and the members
+// job_mbeg[J] .. job_mend[J]-1 of the member list (member k is series
+// mem_series[k] of the series table).  Members of a job are contiguous and in
+// the job's order, which is the order their samples are added.
 template <typename T>
 struct RoundArgs {
-  const T *centroid;
-  int Lc;
+  const T *centroids;
+  const unsigned long long *coff;
+  const int *clen;
+  const int *jflags;
+  const int *mbeg, *mend;
+  int njobs;
   const T *series;
   const uint64_t *offsets;
   const uint64_t *lens;
-  int n, os, oe;
+  const int *mseries, *mjob, *order;
+  int nmem;
   unsigned long long *counter;
   unsigned long long *path_off;  // word offset of member k's path
   unsigned long long *trip_off;  // triple offset of member k's path listing
+  unsigned long long *rng_off;   // offset of member k's per-centroid-index ranges
   int *shortcut;                 // first column of the open-end shortcut, or 0
-  int2 *ranges;                  // [n][Lc] contiguous member-sample range per centroid index
+  int2 *ranges;
   T *edges;
   unsigned long long edge_stride;
   unsigned long long *words;
-  T *mean;
+  T *means;
   uint32_t *counts;
-  double *delta;
-  int32_t *triples;              // optional path listing (i, j, move) per member
+  double *deltas;
+  int32_t *triples;
   int64_t *triple_counts;
 };
 
 template <typename T>
+__device__ __forceinline__ MemberGeom geom_of(const RoundArgs<T> &a, int k, int &job) {
+  job = a.mjob[k];
+  const int f = a.jflags[job];
+  return member_geom<T>(a.lens[a.mseries[k]], uint64_t(a.clen[job]), f & 1, (f >> 1) & 1);
+}
+
+template <typename T>
 __global__ void plan_kernel(RoundArgs<T> a) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned long long w = 0, p = 0;
-  for (int k = 0; k < a.n; ++k) {
-    const MemberGeom g = member_geom<T>(a.lens[k], a.Lc, a.os, a.oe);
+  unsigned long long w = 0, p = 0, r = 0;
+  for (int k = 0; k < a.nmem; ++k) {
+    int job;
+    const MemberGeom g = geom_of<T>(a, k, job);
     a.path_off[k] = w;
     a.trip_off[k] = p;
+    a.rng_off[k] = r;
     w += g.words;
     p += (unsigned long long)(g.m + g.n + 1);
+    r += (unsigned long long)a.clen[job];
   }
+  for (int j = 0; j < a.njobs; ++j)
+    if (a.jflags[j] & 4) a.deltas[j] = 0.0;
 }
 
 __global__ void fill_ranges_kernel(int2 *r, unsigned long long count) {
@@ -127,20 +150,25 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
     unsigned long long q = 0;
     if (lane == 0) q = atomicAdd(a.counter, 1ull);
     q = __shfl_sync(kFull, q, 0);
-    if (q >= (unsigned long long)a.n) break;
-    const int k = a.n - 1 - int(q);  // longest members first when sorted by length
-    const uint64_t len = a.lens[k];
-    const MemberGeom g = member_geom<T>(len, a.Lc, a.os, a.oe);
-    const T *seq = a.series + a.offsets[k];
+    if (q >= (unsigned long long)a.nmem) break;
+    // longest members first when the caller's order (or member order) is by length
+    const int k = a.order ? a.order[q] : a.nmem - 1 - int(q);
+    int jb;
+    const MemberGeom g = geom_of<T>(a, k, jb);
+    const int flags = a.jflags[jb];
+    if (!(flags & 4)) continue;
+    const int os = flags & 1, oe = (flags >> 1) & 1;
+    const T *seq = a.series + a.offsets[a.mseries[k]];
+    const T *cen = a.centroids + a.coff[jb];
     SwathJob<T> job;
-    job.x = g.flip ? a.centroid : seq;
-    job.y = g.flip ? seq : a.centroid;
+    job.x = g.flip ? cen : seq;
+    job.y = g.flip ? seq : cen;
     job.m = g.m;
     job.n = g.n;
     job.r0 = g.r0;
-    job.open_end = a.oe != 0;
+    job.open_end = oe != 0;
     int shortcut = 0;
-    const bool check_short = a.oe && !a.os;
+    const bool check_short = oe && !os;
     for (int s = 0; s < g.swaths; ++s) {
       const int c0 = s * W;
       const bool last = s == g.swaths - 1;
@@ -190,7 +218,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
 
 // Decodes the reference's move at (r, c) of member geometry g.
 template <typename T>
-__device__ __forceinline__ int move_at(const RoundArgs<T> &a, const MemberGeom &g,
+__device__ __forceinline__ int move_at(const MemberGeom &g, int os, int oe,
                                        const unsigned long long *w, int shortcut, int r, int c,
                                        unsigned long long &cache_idx,
                                        unsigned long long &cache_word) {
@@ -198,8 +226,8 @@ __device__ __forceinline__ int move_at(const RoundArgs<T> &a, const MemberGeom &
   // row is row 0 (dtw.hpp:105-108 runs before the row-0 loop)
   if (shortcut && r == g.m - 1 && c >= shortcut) return kMoveOpenRight;
   if (r == 0) {
-    if (c == 0) return a.os ? kMoveNilOpenRight : kMaxMoveNil;
-    return a.os ? kMoveOpenRight : kMoveRight;
+    if (c == 0) return os ? kMoveNilOpenRight : kMaxMoveNil;
+    return os ? kMoveOpenRight : kMoveRight;
   }
   constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
   const int s = c / W;
@@ -221,18 +249,22 @@ __device__ __forceinline__ int move_at(const RoundArgs<T> &a, const MemberGeom &
     cache_idx = idx;
   }
   const int code = int((cache_word >> (2 * j)) & 3ull);
-  if (code == kMoveRight && a.oe && r == g.m - 1) return kMoveOpenRight;
+  if (code == kMoveRight && oe && r == g.m - 1) return kMoveOpenRight;
   return code;
 }
 
 template <typename T>
 __global__ void backtrack_kernel(RoundArgs<T> a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.n) return;
-  const MemberGeom g = member_geom<T>(a.lens[k], a.Lc, a.os, a.oe);
+  if (k >= a.nmem) return;
+  int jb;
+  const MemberGeom g = geom_of<T>(a, k, jb);
+  const int flags = a.jflags[jb];
+  if (!(flags & 4)) return;
+  const int os = flags & 1, oe = (flags >> 1) & 1;
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
-  int2 *rg = a.ranges + (unsigned long long)k * a.Lc;
+  int2 *rg = a.ranges + a.rng_off[k];
   int32_t *tri = a.triples ? a.triples + 3ull * a.trip_off[k] : nullptr;
   long long nt = 0;
   int r = g.m - 1, c = g.n - 1;
@@ -250,7 +282,7 @@ __global__ void backtrack_kernel(RoundArgs<T> a) {
       lo = mi;  // the walk only moves toward smaller indices
     }
   };
-  int mv = move_at<T>(a, g, w, shortcut, r, c, cache_idx, cache_word);
+  int mv = move_at<T>(g, os, oe, w, shortcut, r, c, cache_idx, cache_word);
   // A path has at most m + n - 1 cells and never leaves the matrix; the checks
   // only keep a corrupt path buffer from turning into an endless or
   // out-of-bounds walk (the member is then reported with a count of -1).
@@ -279,7 +311,7 @@ __global__ void backtrack_kernel(RoundArgs<T> a) {
       if (a.triple_counts) a.triple_counts[k] = -1;
       return;
     }
-    mv = move_at<T>(a, g, w, shortcut, r, c, cache_idx, cache_word);
+    mv = move_at<T>(g, os, oe, w, shortcut, r, c, cache_idx, cache_word);
   }
   // the start cell (dba.hpp:412-415)
   if (mv != kMoveNilOpenRight) contribute(0, 0);
@@ -314,25 +346,29 @@ __device__ __forceinline__ double div_rn<double>(double a, double b) { return __
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
+// grid: (ceil(max centroid length / 256), jobs)
 template <typename T>
-__global__ void reduce_kernel(RoundArgs<T> a, double *block_max) {
+__global__ void reduce_kernel(RoundArgs<T> a) {
   __shared__ double smax[256];
+  const int jb = blockIdx.y;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Lc = a.clen[jb];
+  const bool live = (a.jflags[jb] & 4) != 0;
   double dl = 0.0;
-  if (t < a.Lc) {
+  if (live && t < Lc) {
     T sum = T(0);
     uint32_t cnt = 0;
-    for (int k = 0; k < a.n; ++k) {
-      const int2 r = a.ranges[(unsigned long long)k * a.Lc + t];
+    for (int k = a.mbeg[jb]; k < a.mend[jb]; ++k) {
+      const int2 r = a.ranges[a.rng_off[k] + t];
       if (r.y < r.x) continue;
-      const T *seq = a.series + a.offsets[k];
+      const T *seq = a.series + a.offsets[a.mseries[k]];
       for (int i = r.y; i >= r.x; --i) sum = add_rn(sum, seq[i]);
       cnt += uint32_t(r.y - r.x + 1);
     }
     const T mean = cnt ? div_rn<T>(sum, T(cnt)) : host_default_nan<T>();
-    a.mean[t] = mean;
-    a.counts[t] = cnt;
-    const double d = fabs(double(a.centroid[t] - mean));
+    a.means[a.coff[jb] + t] = mean;
+    a.counts[a.coff[jb] + t] = cnt;
+    const double d = fabs(double(a.centroids[a.coff[jb] + t] - mean));
     dl = d > 0.0 ? d : 0.0;  // NaN never raises the maximum (dba.hpp:833)
   }
   smax[threadIdx.x] = dl;
@@ -342,14 +378,26 @@ __global__ void reduce_kernel(RoundArgs<T> a, double *block_max) {
       smax[threadIdx.x] = smax[threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0) block_max[blockIdx.x] = smax[0];
+  // non-negative doubles order like their bit patterns
+  if (threadIdx.x == 0 && live)
+    atomicMax(reinterpret_cast<unsigned long long *>(a.deltas + jb),
+              (unsigned long long)__double_as_longlong(smax[0]));
 }
 
-__global__ void final_max_kernel(const double *block_max, int nb, double *out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double m = 0.0;
-  for (int i = 0; i < nb; ++i) m = block_max[i] > m ? block_max[i] : m;
-  *out = m;
+// One job, members 0..n-1 in order (the single-cluster DBAUpdate call).
+__global__ void single_job_kernel(int *mseries, int *mjob, int n, int *clen, int Lc, int *jflags,
+                                  int flags, int *mbeg, int *mend, unsigned long long *coff) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    mseries[k] = k;
+    mjob[k] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    clen[0] = Lc;
+    jflags[0] = flags;
+    mbeg[0] = 0;
+    mend[0] = n;
+    coff[0] = 0;
+  }
 }
 
 template <typename T>
@@ -369,42 +417,85 @@ int round_grid() {
 }
 
 struct RoundLayout {
-  size_t off_counter, off_path, off_trip, off_short, off_ranges, off_blockmax, off_edges, off_words,
-      total;
+  size_t off_counter, off_path, off_trip, off_rng, off_short, off_single, off_ranges, off_edges,
+      off_words, total;
   unsigned long long edge_stride;
 };
 
+// Workspace layout for nmem members / njobs jobs with the given totals.
 template <typename T>
-RoundLayout round_layout(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe) {
+RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
+                         unsigned long long ranges, unsigned long long maxm) {
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-  unsigned long long words = 0, maxm = Lc;
-  for (int k = 0; k < n; ++k) {
-    const MemberGeom g = member_geom<T>(h_lens[k], Lc, os, oe);
-    words += g.words;
-    if ((unsigned long long)g.m > maxm) maxm = g.m;
-  }
   RoundLayout L;
   L.edge_stride = (maxm + 32 + 31) / 32 * 32;
   const size_t slots = size_t(round_grid<T>()) * kRoundWarps;
-  const int nb = int((Lc + 255) / 256);
   size_t o = 0;
   L.off_counter = o; o += 256;
-  L.off_path = o; o += up(size_t(n) * 8);
-  L.off_trip = o; o += up(size_t(n) * 8);
-  L.off_short = o; o += up(size_t(n) * 4);
-  L.off_ranges = o; o += up(size_t(n) * Lc * sizeof(int2));
-  L.off_blockmax = o; o += up(size_t(nb) * 8);
+  L.off_path = o; o += up(size_t(nmem) * 8);
+  L.off_trip = o; o += up(size_t(nmem) * 8);
+  L.off_rng = o; o += up(size_t(nmem) * 8);
+  L.off_short = o; o += up(size_t(nmem) * 4);
+  // single-job descriptors: mseries, mjob (nmem ints each), clen, jflags, mbeg, mend, coff
+  L.off_single = o; o += up(size_t(nmem) * 8 + 64);
+  L.off_ranges = o; o += up(size_t(ranges) * sizeof(int2));
   L.off_edges = o; o += up(slots * 2 * L.edge_stride * sizeof(T));
   L.off_words = o; o += up(words * 8);
   L.total = o;
+  (void)njobs;
   return L;
+}
+
+template <typename T>
+void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint64_t *h_clen,
+                 const int *h_flags, unsigned long long &words, unsigned long long &ranges,
+                 unsigned long long &maxm) {
+  words = ranges = 0;
+  maxm = 1;
+  for (int k = 0; k < nmem; ++k) {
+    const int j = h_mjob ? h_mjob[k] : 0;
+    const int f = h_flags[j];
+    const MemberGeom g = member_geom<T>(h_lens[k], h_clen[j], f & 1, (f >> 1) & 1);
+    words += g.words;
+    ranges += h_clen[j];
+    if ((unsigned long long)g.m > maxm) maxm = g.m;
+  }
+}
+
+template <typename T>
+int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen,
+                 cudaStream_t stream) {
+  a.counter = reinterpret_cast<unsigned long long *>(base + L.off_counter);
+  a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
+  a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
+  a.rng_off = reinterpret_cast<unsigned long long *>(base + L.off_rng);
+  a.shortcut = reinterpret_cast<int *>(base + L.off_short);
+  a.ranges = reinterpret_cast<int2 *>(base + L.off_ranges);
+  a.edges = reinterpret_cast<T *>(base + L.off_edges);
+  a.edge_stride = L.edge_stride;
+  a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
+  const unsigned long long nr = (L.off_edges - L.off_ranges) / sizeof(int2);
+  cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
+  plan_kernel<T><<<1, 32, 0, stream>>>(a);
+  fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
+  path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>
+      <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
+  backtrack_kernel<T><<<(a.nmem + 127) / 128, 128, 0, stream>>>(a);
+  dim3 rg((max_clen + 255) / 256, a.njobs);
+  reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
+  return check_launch("DBA round kernels");
 }
 
 }  // namespace
 
 template <typename T>
 size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe) {
-  return round_layout<T>(h_lens, n, Lc, os, oe).total;
+  unsigned long long words, ranges, maxm;
+  const uint64_t clen = Lc;
+  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm);
+  if (Lc > maxm) maxm = Lc;
+  return round_layout<T>(n, 1, words, ranges, maxm).total;
 }
 
 template <typename T>
@@ -412,44 +503,90 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
                      const uint64_t *lens, const uint64_t *h_lens, int n, int os, int oe, T *mean,
                      uint32_t *counts, double *delta, int32_t *triples, int64_t *triple_counts,
                      void *ws, size_t ws_bytes, cudaStream_t stream) {
-  const RoundLayout L = round_layout<T>(h_lens, n, Lc, os, oe);
+  unsigned long long words, ranges, maxm;
+  const uint64_t clen = Lc;
+  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm);
+  if (Lc > maxm) maxm = Lc;
+  const RoundLayout L = round_layout<T>(n, 1, words, ranges, maxm);
   if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA round workspace too small");
   char *base = static_cast<char *>(ws);
+  int *single = reinterpret_cast<int *>(base + L.off_single);
+  int *mseries = single, *mjob = single + n, *d_clen = single + 2 * n, *d_flags = single + 2 * n + 1,
+      *d_mbeg = single + 2 * n + 2, *d_mend = single + 2 * n + 3;
+  unsigned long long *d_coff =
+      reinterpret_cast<unsigned long long *>(base + L.off_single + ((size_t(2 * n + 4) * 4 + 7) / 8) * 8);
+  single_job_kernel<<<(n + 255) / 256, 256, 0, stream>>>(mseries, mjob, n, d_clen, int(Lc), d_flags,
+                                                        flags, d_mbeg, d_mend, d_coff);
   RoundArgs<T> a;
-  a.centroid = centroid;
-  a.Lc = int(Lc);
+  a.centroids = centroid;
+  a.coff = d_coff;
+  a.clen = d_clen;
+  a.jflags = d_flags;
+  a.mbeg = d_mbeg;
+  a.mend = d_mend;
+  a.njobs = 1;
   a.series = series;
   a.offsets = offsets;
   a.lens = lens;
-  a.n = n;
-  a.os = os ? 1 : 0;
-  a.oe = oe ? 1 : 0;
-  a.counter = reinterpret_cast<unsigned long long *>(base + L.off_counter);
-  a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
-  a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
-  a.shortcut = reinterpret_cast<int *>(base + L.off_short);
-  a.ranges = reinterpret_cast<int2 *>(base + L.off_ranges);
-  a.edges = reinterpret_cast<T *>(base + L.off_edges);
-  a.edge_stride = L.edge_stride;
-  a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
-  a.mean = mean;
+  a.mseries = mseries;
+  a.mjob = mjob;
+  a.order = nullptr;
+  a.nmem = n;
+  a.means = mean;
   a.counts = counts;
-  a.delta = delta;
+  a.deltas = delta;
   a.triples = triples;
   a.triple_counts = triple_counts;
-  double *bmax = reinterpret_cast<double *>(base + L.off_blockmax);
-  const int nb = int((Lc + 255) / 256);
-  cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
-  plan_kernel<T><<<1, 32, 0, stream>>>(a);
-  const unsigned long long nr = (unsigned long long)n * Lc;
-  fill_ranges_kernel<<<nr > 0 ? int((nr + 255) / 256 < 4096 ? (nr + 255) / 256 : 4096) : 1, 256, 0,
-                       stream>>>(a.ranges, nr);
-  path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>
-      <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
-  backtrack_kernel<T><<<(n + 127) / 128, 128, 0, stream>>>(a);
-  reduce_kernel<T><<<nb, 256, 0, stream>>>(a, bmax);
-  final_max_kernel<<<1, 32, 0, stream>>>(bmax, nb, delta);
-  return check_launch("DBA round kernels");
+  return launch_round<T>(a, L, base, int(Lc), stream);
+}
+
+template <typename T>
+size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int nmem,
+                                 const uint64_t *h_clen, const int *h_flags, int njobs) {
+  unsigned long long words, ranges, maxm;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm);
+  for (int j = 0; j < njobs; ++j)
+    if (h_clen[j] > maxm) maxm = h_clen[j];
+  return round_layout<T>(nmem, njobs, words, ranges, maxm).total;
+}
+
+template <typename T>
+int dba_batch_launch(const T *centroids, const unsigned long long *coff, const int *clen,
+                     const int *jflags, const int *mbeg, const int *mend, int njobs, int max_clen,
+                     const T *series, const uint64_t *offsets, const uint64_t *lens,
+                     const int *mseries, const int *mjob, const int *order, int nmem,
+                     const uint64_t *h_mlens, const int *h_mjob, const uint64_t *h_clen,
+                     const int *h_flags, T *means, uint32_t *counts, double *deltas,
+                     int32_t *triples, int64_t *triple_counts, void *ws, size_t ws_bytes,
+                     cudaStream_t stream) {
+  unsigned long long words, ranges, maxm;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm);
+  for (int j = 0; j < njobs; ++j)
+    if (h_clen[j] > maxm) maxm = h_clen[j];
+  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm);
+  if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA batch workspace too small");
+  RoundArgs<T> a;
+  a.centroids = centroids;
+  a.coff = coff;
+  a.clen = clen;
+  a.jflags = jflags;
+  a.mbeg = mbeg;
+  a.mend = mend;
+  a.njobs = njobs;
+  a.series = series;
+  a.offsets = offsets;
+  a.lens = lens;
+  a.mseries = mseries;
+  a.mjob = mjob;
+  a.order = order;
+  a.nmem = nmem;
+  a.means = means;
+  a.counts = counts;
+  a.deltas = deltas;
+  a.triples = triples;
+  a.triple_counts = triple_counts;
+  return launch_round<T>(a, L, static_cast<char *>(ws), max_clen, stream);
 }
 
 template size_t dba_round_workspace_bytes<float>(const uint64_t *, int, uint64_t, int, int);
@@ -462,5 +599,23 @@ template int dba_round_launch<double>(const double *, uint64_t, const double *, 
                                       const uint64_t *, const uint64_t *, int, int, int, double *,
                                       uint32_t *, double *, int32_t *, int64_t *, void *, size_t,
                                       cudaStream_t);
+template size_t dba_batch_workspace_bytes<float>(const uint64_t *, const int *, int,
+                                                 const uint64_t *, const int *, int);
+template size_t dba_batch_workspace_bytes<double>(const uint64_t *, const int *, int,
+                                                  const uint64_t *, const int *, int);
+template int dba_batch_launch<float>(const float *, const unsigned long long *, const int *,
+                                     const int *, const int *, const int *, int, int,
+                                     const float *, const uint64_t *, const uint64_t *,
+                                     const int *, const int *, const int *, int, const uint64_t *,
+                                     const int *, const uint64_t *, const int *, float *,
+                                     uint32_t *, double *, int32_t *, int64_t *, void *, size_t,
+                                     cudaStream_t);
+template int dba_batch_launch<double>(const double *, const unsigned long long *, const int *,
+                                      const int *, const int *, const int *, int, int,
+                                      const double *, const uint64_t *, const uint64_t *,
+                                      const int *, const int *, const int *, int,
+                                      const uint64_t *, const int *, const uint64_t *, const int *,
+                                      double *, uint32_t *, double *, int32_t *, int64_t *, void *,
+                                      size_t, cudaStream_t);
 
 }  // namespace odba

@@ -312,3 +312,71 @@ extern "C" int odba_dtw_pairwise_noalloc_f32(const float *series, const uint64_t
   return odba::pairwise_noalloc<float>(series, offsets, lens, n, max_len, use_open_start,
                                        use_open_end, dists, static_cast<cudaStream_t>(stream));
 }
+
+// ---------------------------------------------------------------------------
+// Pairs from a task list: many independent jobs (each its own set of series,
+// its own alignment mode) in one persistent launch.  The caller orders the
+// tasks (largest m*n first keeps the tail short); each warp takes the next
+// task from the device counter.
+namespace odba {
+namespace {
+
+template <typename T, int RF, int RQ>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
+    pairlist_kernel(const T *series, const uint64_t *offsets, const uint64_t *lens,
+                    const odba_pair_task *tasks, unsigned long long ntasks, T *dists,
+                    unsigned long long *counter, T *edges, unsigned long long edge_stride) {
+  const int lane = threadIdx.x & 31;
+  const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  T *e0 = edges + slot * 2 * edge_stride;
+  T *e1 = e0 + edge_stride;
+  for (;;) {
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(counter, 1ull);
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= ntasks) break;
+    const odba_pair_task task = tasks[q];
+    const int os = int((task.out >> 62) & 1ull), oe = int((task.out >> 63) & 1ull);
+    const unsigned long long out = task.out & ((1ull << 62) - 1);
+    SwathJob<T> job;
+    job.x = series + offsets[task.first];
+    job.m = int(lens[task.first]);
+    job.y = series + offsets[task.second];
+    job.n = int(lens[task.second]);
+    job.r0 = os;
+    job.open_end = oe != 0;
+    T corner = T(0);
+    sweep_pair<T, RF, RQ>(job, e0, e1, corner);
+    if (lane == 0) dists[out] = pair_distance<T>(corner, job.m, job.n, os, oe);
+  }
+}
+
+}  // namespace
+
+template <typename T>
+int pairlist_launch(const T *series, const uint64_t *offsets, const uint64_t *lens,
+                    const odba_pair_task *tasks, unsigned long long ntasks, uint64_t max_len,
+                    T *dists, void *workspace, size_t ws_bytes, cudaStream_t stream) {
+  if (ntasks == 0) return ODBA_OK;
+  const size_t need = pairwise_workspace_bytes<T>(max_len);
+  if (ws_bytes < need) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "workspace too small");
+  auto *counter = static_cast<unsigned long long *>(workspace);
+  T *edges = reinterpret_cast<T *>(static_cast<char *>(workspace) + 256);
+  const unsigned long long stride = (max_len + 32 + 31) / 32 * 32;
+  cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+  unsigned long long blocks = (ntasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  int grid = grid_size<T>();
+  if (blocks < (unsigned long long)grid) grid = int(blocks);
+  pairlist_kernel<T, Tune<T>::RF, Tune<T>::RQ><<<grid, kWarpsPerBlock * 32, 0, stream>>>(
+      series, offsets, lens, tasks, ntasks, dists, counter, edges, stride);
+  return check_launch("pair-list DTW kernel");
+}
+
+template int pairlist_launch<float>(const float *, const uint64_t *, const uint64_t *,
+                                    const odba_pair_task *, unsigned long long, uint64_t, float *,
+                                    void *, size_t, cudaStream_t);
+template int pairlist_launch<double>(const double *, const uint64_t *, const uint64_t *,
+                                     const odba_pair_task *, unsigned long long, uint64_t,
+                                     double *, void *, size_t, cudaStream_t);
+
+}  // namespace odba

@@ -1150,3 +1150,364 @@ extern "C" int odba_segment_host_f64(const double *h_series, const uint64_t *h_l
     return ODBA_ERR_INVALID_ARGUMENT;
   return segment_host<double>(h_series, h_lens, n, min_segment_length, prefix_skip, h_out, h_out_lens);
 }
+
+// ---------------------------------------------------------------------------
+// Many independent DBA jobs (one cluster each, cdist 1, no files): every job is
+// what performDBA computes for its series -- truncation, stable length sort,
+// z-norm, medoid, rounds to delta 0 / flip-flop / 250 rounds, rescale -- but
+// run either batched (all pairs of all jobs in one length-sorted launch; one
+// DBA round for all unconverged jobs per CUDA graph replay) or plain (job by
+// job through the single-job entry points, the drop-in path).
+
+namespace {
+
+template <typename T>
+struct JobSet {
+  int njobs = 0;
+  std::vector<int> jbeg, jend, flags;         // series range per job in the sorted table
+  std::vector<std::vector<int>> order;        // per job: sorted position -> input position
+  DeviceSet<T> ds;                            // all jobs' series, sorted within each job
+};
+
+// Truncation and stable sort per job (dba.hpp:868-885), then upload.
+template <typename T>
+void build_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, const int *job_end,
+                const int *job_flags, int njobs, JobSet<T> &js, cudaStream_t st) {
+  js.njobs = njobs;
+  js.jbeg.assign(njobs, 0);
+  js.jend.assign(njobs, 0);
+  js.flags.assign(job_flags, job_flags + njobs);
+  js.order.assign(njobs, {});
+  std::vector<uint64_t> offs;
+  uint64_t acc = 0;
+  for (int j = 0; j < njobs; ++j) {
+    (void)0;
+  }
+  // input offsets of every series
+  int total = 0;
+  for (int j = 0; j < njobs; ++j) total = std::max(total, job_end[j]);
+  offs.assign(total, 0);
+  for (int i = 0; i < total; ++i) {
+    offs[i] = acc;
+    acc += h_lens[i];
+  }
+  std::vector<T *> ptrs;
+  std::vector<size_t> lens;
+  for (int j = 0; j < njobs; ++j) {
+    const int b = job_begin[j], e = job_end[j];
+    std::vector<int> idx(e - b);
+    std::vector<size_t> L(e - b);
+    for (int i = b; i < e; ++i) {
+      idx[i - b] = i - b;
+      size_t len = h_lens[i];
+      if (len && h_series[offs[i] + len - 1] >= std::sqrt(std::numeric_limits<T>::max())) --len;
+      L[i - b] = len;
+    }
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return L[a] < L[c]; });
+    js.jbeg[j] = int(ptrs.size());
+    for (int k : idx) {
+      ptrs.push_back(const_cast<T *>(h_series + offs[b + k]));
+      lens.push_back(L[k]);
+    }
+    js.jend[j] = int(ptrs.size());
+    js.order[j] = idx;
+  }
+  js.ds.upload(ptrs.data(), lens.data(), int(ptrs.size()), st);
+}
+
+template <typename T>
+bool flip_flop_or_done(double delta, int round, bool open, std::vector<T> &nb, std::vector<T> &prev,
+                       std::vector<T> &two_prev) {
+  if (delta == 0) return true;
+  if (open) {
+    if (round >= 1 && !std::memcmp(nb.data(), two_prev.data(), sizeof(T) * nb.size())) return true;
+    if (round > 1) two_prev = prev;
+    if (round > 0) prev = nb;
+  }
+  return false;
+}
+
+template <typename T>
+int run_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, const int *job_end,
+             const int *job_flags, int njobs, int norm, int max_rounds, bool batched,
+             int *h_medoids, uint64_t *h_centroid_offsets, T *h_centroids, int *h_rounds,
+             double *h_deltas, cudaStream_t st) {
+  JobSet<T> js;
+  build_jobs<T>(h_series, h_lens, job_begin, job_end, job_flags, njobs, js, st);
+  const int n = js.ds.n;
+  DevBuf d_means(std::max(1, n) * sizeof(double)), d_sig(std::max(1, n) * sizeof(double));
+  std::vector<double> means(n, 0.0), sigmas(n, 1.0);
+  if (norm) {
+    check(Ops<T>::znorm(ptr<T>(js.ds.data), ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens), n,
+                        ptr<double>(d_means), ptr<double>(d_sig), st),
+          "z-normalisation");
+    check_cuda(cudaMemcpyAsync(means.data(), d_means.p, n * sizeof(double), cudaMemcpyDeviceToHost, st), "means");
+    check_cuda(cudaMemcpyAsync(sigmas.data(), d_sig.p, n * sizeof(double), cudaMemcpyDeviceToHost, st), "sigmas");
+  }
+  // ---- medoids
+  std::vector<unsigned long long> tri_off(njobs + 1, 0);
+  for (int j = 0; j < njobs; ++j) {
+    const unsigned long long m = (unsigned long long)(js.jend[j] - js.jbeg[j]);
+    tri_off[j + 1] = tri_off[j] + m * (m - 1) / 2;
+  }
+  DevBuf d_dists(std::max<unsigned long long>(tri_off[njobs], 1) * sizeof(T));
+  DevBuf d_sos(std::max(1, n) * sizeof(T)), d_med(std::max(1, njobs) * sizeof(int));
+  DevBuf ws(odba_dtw_pairwise_workspace_bytes(sizeof(T), std::max<uint64_t>(js.ds.max_len, 1)));
+  if (batched) {
+    // one launch for every pair of every job, largest m*n first
+    std::vector<odba_pair_task> tasks;
+    tasks.reserve(tri_off[njobs]);
+    std::vector<double> cost;
+    cost.reserve(tri_off[njobs]);
+    for (int j = 0; j < njobs; ++j) {
+      const int b = js.jbeg[j], m = js.jend[j] - js.jbeg[j];
+      const uint64_t fl = (uint64_t(js.flags[j] & 1) << 62) | (uint64_t((js.flags[j] >> 1) & 1) << 63);
+      unsigned long long p = tri_off[j];
+      for (int s = 0; s + 1 < m; ++s)
+        for (int t = s + 1; t < m; ++t) {
+          tasks.push_back(odba_pair_task{uint32_t(b + s), uint32_t(b + t), p | fl});
+          cost.push_back(double(js.ds.h_lens[b + s]) * double(js.ds.h_lens[b + t]));
+          ++p;
+        }
+    }
+    std::vector<size_t> perm(tasks.size());
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+    std::vector<odba_pair_task> sorted(tasks.size());
+    for (size_t i = 0; i < perm.size(); ++i) sorted[i] = tasks[perm[i]];
+    DevBuf d_tasks(std::max<size_t>(sorted.size(), 1) * sizeof(odba_pair_task));
+    check_cuda(cudaMemcpyAsync(d_tasks.p, sorted.data(), sorted.size() * sizeof(odba_pair_task),
+                               cudaMemcpyHostToDevice, st), "task upload");
+    if (!sorted.empty())
+      check(sizeof(T) == 4
+                ? odba_dtw_pairlist_f32((const float *)js.ds.data.p, ptr<uint64_t>(js.ds.offs),
+                                        ptr<uint64_t>(js.ds.lens), ptr<odba_pair_task>(d_tasks),
+                                        sorted.size(), js.ds.max_len, (float *)d_dists.p, ws.p,
+                                        ws.bytes, st)
+                : odba_dtw_pairlist_f64((const double *)js.ds.data.p, ptr<uint64_t>(js.ds.offs),
+                                        ptr<uint64_t>(js.ds.lens), ptr<odba_pair_task>(d_tasks),
+                                        sorted.size(), js.ds.max_len, (double *)d_dists.p, ws.p,
+                                        ws.bytes, st),
+            "pair-list DTW");
+    check_cuda(cudaStreamSynchronize(st), "pair-list DTW");
+  }
+  for (int j = 0; j < njobs; ++j) {
+    const int b = js.jbeg[j], m = js.jend[j] - js.jbeg[j];
+    if (m < 1) continue;
+    if (!batched && m >= 2)
+      check(Ops<T>::pairwise(ptr<T>(js.ds.data), ptr<uint64_t>(js.ds.offs) + b,
+                             ptr<uint64_t>(js.ds.lens) + b, m, js.ds.max_len, js.flags[j] & 1,
+                             (js.flags[j] >> 1) & 1, ptr<T>(d_dists) + tri_off[j], ws.p, ws.bytes, st),
+            "all-pairs DTW");
+    check(sizeof(T) == 4
+              ? odba_medoid_f32((const float *)d_dists.p + tri_off[j], ptr<uint64_t>(js.ds.lens) + b,
+                                m, (float *)d_sos.p + b, ptr<int>(d_med) + j, st)
+              : odba_medoid_f64((const double *)d_dists.p + tri_off[j], ptr<uint64_t>(js.ds.lens) + b,
+                                m, (double *)d_sos.p + b, ptr<int>(d_med) + j, st),
+          "medoid");
+    if (!batched) check_cuda(cudaStreamSynchronize(st), "medoid");
+  }
+  std::vector<int> med(njobs, 0);
+  check_cuda(cudaMemcpyAsync(med.data(), d_med.p, njobs * sizeof(int), cudaMemcpyDeviceToHost, st), "medoid download");
+  check_cuda(cudaStreamSynchronize(st), "medoids");
+  // ---- rounds
+  std::vector<uint64_t> coff(njobs, 0);
+  std::vector<int> clen(njobs, 0);
+  uint64_t ctot = 0;
+  int max_clen = 1;
+  for (int j = 0; j < njobs; ++j) {
+    const int mi = js.jbeg[j] + med[j];
+    coff[j] = ctot;
+    clen[j] = int(js.ds.h_lens[mi]);
+    ctot += clen[j];
+    max_clen = std::max(max_clen, clen[j]);
+    h_medoids[j] = js.order[j][med[j]];
+    h_centroid_offsets[j] = coff[j];
+  }
+  DevBuf cbuf[2] = {DevBuf(std::max<uint64_t>(ctot, 1) * sizeof(T)), DevBuf(std::max<uint64_t>(ctot, 1) * sizeof(T))};
+  DevBuf d_counts(std::max<uint64_t>(ctot, 1) * sizeof(uint32_t)), d_deltas(njobs * sizeof(double));
+  for (int j = 0; j < njobs; ++j)
+    check_cuda(cudaMemcpyAsync(ptr<T>(cbuf[0]) + coff[j], ptr<T>(js.ds.data) + js.ds.h_offs[js.jbeg[j] + med[j]],
+                               clen[j] * sizeof(T), cudaMemcpyDeviceToDevice, st), "seed centroids");
+  std::vector<T> host_c(ctot);
+  check_cuda(cudaMemcpyAsync(host_c.data(), cbuf[0].p, ctot * sizeof(T), cudaMemcpyDeviceToHost, st), "seed download");
+  check_cuda(cudaStreamSynchronize(st), "seeds");
+  std::vector<int> active(njobs, 0), rounds(njobs, 0);
+  std::vector<double> deltas(njobs, 0.0);
+  std::vector<std::vector<T>> prev(njobs), two_prev(njobs);
+  int live = 0;
+  for (int j = 0; j < njobs; ++j) {
+    if (js.jend[j] - js.jbeg[j] > 1) {
+      active[j] = 1;
+      ++live;
+      prev[j].assign(clen[j], T(0));
+      two_prev[j].assign(clen[j], T(0));
+    }
+  }
+  // member tables: member k of job j is series jbeg[j] + k, in sorted order
+  std::vector<int> mseries(n), mjob(n), mbeg(njobs), mend(njobs), h_flags(njobs);
+  std::vector<uint64_t> h_mlens(n), h_clen(njobs);
+  for (int j = 0; j < njobs; ++j) {
+    mbeg[j] = js.jbeg[j];
+    mend[j] = js.jend[j];
+    h_clen[j] = uint64_t(clen[j]);
+    for (int k = js.jbeg[j]; k < js.jend[j]; ++k) {
+      mseries[k] = k;
+      mjob[k] = j;
+      h_mlens[k] = js.ds.h_lens[k];
+    }
+  }
+  std::vector<int> morder(n);
+  std::iota(morder.begin(), morder.end(), 0);
+  std::stable_sort(morder.begin(), morder.end(), [&](int a, int b) {
+    return double(h_mlens[a]) * h_clen[mjob[a]] > double(h_mlens[b]) * h_clen[mjob[b]];
+  });
+  auto flags_now = [&]() {
+    for (int j = 0; j < njobs; ++j) h_flags[j] = (js.flags[j] & 3) | (active[j] ? 4 : 0);
+  };
+  flags_now();
+  DevBuf d_mseries(n * sizeof(int)), d_mjob(n * sizeof(int)), d_mbeg(njobs * sizeof(int)),
+      d_mend(njobs * sizeof(int)), d_flags(njobs * sizeof(int)), d_clen(njobs * sizeof(int)),
+      d_coff(njobs * sizeof(uint64_t)), d_order(n * sizeof(int));
+  check_cuda(cudaMemcpyAsync(d_mseries.p, mseries.data(), n * sizeof(int), cudaMemcpyHostToDevice, st), "members");
+  check_cuda(cudaMemcpyAsync(d_mjob.p, mjob.data(), n * sizeof(int), cudaMemcpyHostToDevice, st), "members");
+  check_cuda(cudaMemcpyAsync(d_mbeg.p, mbeg.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "jobs");
+  check_cuda(cudaMemcpyAsync(d_mend.p, mend.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "jobs");
+  check_cuda(cudaMemcpyAsync(d_clen.p, clen.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "jobs");
+  check_cuda(cudaMemcpyAsync(d_coff.p, coff.data(), njobs * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "jobs");
+  check_cuda(cudaMemcpyAsync(d_order.p, morder.data(), n * sizeof(int), cudaMemcpyHostToDevice, st), "members");
+  check_cuda(cudaMemcpyAsync(d_flags.p, h_flags.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "flags");
+  std::vector<T> nb(ctot);
+  if (batched && live) {
+    // all flags active for sizing (inactive jobs only skip work)
+    std::vector<int> size_flags(njobs);
+    for (int j = 0; j < njobs; ++j) size_flags[j] = (js.flags[j] & 3) | 4;
+    DevBuf rws(odba_dba_batch_workspace_bytes(sizeof(T), h_mlens.data(), mjob.data(), n, h_clen.data(),
+                                              size_flags.data(), njobs));
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    for (int g = 0; g < 2; ++g) {
+      cudaGraph_t graph;
+      check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
+      const T *cin = ptr<T>(cbuf[g]);
+      T *cout = ptr<T>(cbuf[1 - g]);
+      const int rc = sizeof(T) == 4
+          ? odba_dba_batch_round_f32((const float *)cin, ptr<uint64_t>(d_coff), ptr<int>(d_clen), ptr<int>(d_flags),
+                                     ptr<int>(d_mbeg), ptr<int>(d_mend), njobs, max_clen,
+                                     (const float *)js.ds.data.p, ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens),
+                                     ptr<int>(d_mseries), ptr<int>(d_mjob), ptr<int>(d_order), n, h_mlens.data(),
+                                     mjob.data(), h_clen.data(), size_flags.data(), (float *)cout,
+                                     ptr<uint32_t>(d_counts), ptr<double>(d_deltas), nullptr, nullptr, rws.p,
+                                     rws.bytes, st)
+          : odba_dba_batch_round_f64((const double *)cin, ptr<uint64_t>(d_coff), ptr<int>(d_clen), ptr<int>(d_flags),
+                                     ptr<int>(d_mbeg), ptr<int>(d_mend), njobs, max_clen,
+                                     (const double *)js.ds.data.p, ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens),
+                                     ptr<int>(d_mseries), ptr<int>(d_mjob), ptr<int>(d_order), n, h_mlens.data(),
+                                     mjob.data(), h_clen.data(), size_flags.data(), (double *)cout,
+                                     ptr<uint32_t>(d_counts), ptr<double>(d_deltas), nullptr, nullptr, rws.p,
+                                     rws.bytes, st);
+      check_cuda(cudaStreamEndCapture(st, &graph), "graph capture");
+      check(rc, "batched DBA round (capture)");
+      check_cuda(cudaGraphInstantiate(&exec[g], graph, 0), "graph instantiate");
+      cudaGraphDestroy(graph);
+    }
+    int cur = 0;
+    for (int round = 0; round < max_rounds && live; ++round) {
+      check_cuda(cudaMemcpyAsync(d_flags.p, h_flags.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "flags");
+      check_cuda(cudaGraphLaunch(exec[cur], st), "graph launch");
+      check_cuda(cudaMemcpyAsync(nb.data(), cbuf[1 - cur].p, ctot * sizeof(T), cudaMemcpyDeviceToHost, st), "means");
+      check_cuda(cudaMemcpyAsync(deltas.data(), d_deltas.p, njobs * sizeof(double), cudaMemcpyDeviceToHost, st), "deltas");
+      check_cuda(cudaStreamSynchronize(st), "batched round");
+      for (int j = 0; j < njobs; ++j) {
+        if (!active[j]) continue;
+        rounds[j] = round + 1;
+        std::vector<T> v(nb.begin() + coff[j], nb.begin() + coff[j] + clen[j]);
+        const bool open = (js.flags[j] & 3) != 0;
+        std::copy(v.begin(), v.end(), host_c.begin() + coff[j]);
+        h_deltas[j] = deltas[j];
+        if (flip_flop_or_done<T>(deltas[j], round, open, v, prev[j], two_prev[j])) {
+          active[j] = 0;
+          --live;
+        }
+      }
+      flags_now();
+      // the next round reads the means just written: copy finished jobs'
+      // values along so both buffers agree for them
+      cur = 1 - cur;
+    }
+    for (int g = 0; g < 2; ++g) cudaGraphExecDestroy(exec[g]);
+  } else if (live) {
+    // plain: job by job, one round per call, synchronizing every round (performDBA's loop)
+    for (int j = 0; j < njobs; ++j) {
+      if (!active[j]) continue;
+      const int b = js.jbeg[j], m = js.jend[j] - js.jbeg[j];
+      const int os = js.flags[j] & 1, oe = (js.flags[j] >> 1) & 1;
+      DevBuf rws(odba_dba_round_workspace_bytes(sizeof(T), js.ds.h_lens.data() + b, m, clen[j], os, oe));
+      T *cin = ptr<T>(cbuf[0]) + coff[j];
+      T *cout = ptr<T>(cbuf[1]) + coff[j];
+      std::vector<T> v(clen[j]);
+      for (int round = 0; round < max_rounds; ++round) {
+        check(Ops<T>::round(cin, clen[j], ptr<T>(js.ds.data), ptr<uint64_t>(js.ds.offs) + b,
+                            ptr<uint64_t>(js.ds.lens) + b, js.ds.h_lens.data() + b, m, os, oe, cout,
+                            ptr<uint32_t>(d_counts) + coff[j], ptr<double>(d_deltas) + j, nullptr, nullptr,
+                            rws.p, rws.bytes, st),
+              "DBA round");
+        double delta = 0;
+        check_cuda(cudaMemcpyAsync(v.data(), cout, clen[j] * sizeof(T), cudaMemcpyDeviceToHost, st), "means");
+        check_cuda(cudaMemcpyAsync(&delta, ptr<double>(d_deltas) + j, sizeof(double), cudaMemcpyDeviceToHost, st), "delta");
+        check_cuda(cudaStreamSynchronize(st), "DBA round");
+        rounds[j] = round + 1;
+        h_deltas[j] = delta;
+        std::copy(v.begin(), v.end(), host_c.begin() + coff[j]);
+        if (flip_flop_or_done<T>(delta, round, (js.flags[j] & 3) != 0, v, prev[j], two_prev[j])) break;
+        check_cuda(cudaMemcpyAsync(cin, cout, clen[j] * sizeof(T), cudaMemcpyDeviceToDevice, st), "centroid update");
+      }
+    }
+  }
+  // rescale by the medoid's mean and sigma (dba.hpp:1117-1125) and return
+  for (int j = 0; j < njobs; ++j) {
+    const int mi = js.jbeg[j] + med[j];
+    h_rounds[j] = rounds[j];
+    for (int i = 0; i < clen[j]; ++i) {
+      T v = host_c[coff[j] + i];
+      if (norm) v = (T)(means[mi] + v * sigmas[mi]);
+      h_centroids[coff[j] + i] = v;
+    }
+  }
+  return ODBA_OK;
+}
+
+}  // namespace
+
+#define ODBA_JOBS_ENTRY(SFX, T)                                                                  \
+  extern "C" int odba_dba_jobs_##SFX(const T *h_series, const uint64_t *h_lens,                 \
+                                     const int *job_begin, const int *job_end,                  \
+                                     const int *job_flags, int njobs, int norm, int max_rounds,   \
+                                     int batched, int *h_medoids, uint64_t *h_centroid_offsets,   \
+                                     T *h_centroids, int *h_rounds, double *h_deltas,            \
+                                     void *stream) {                                              \
+    if (njobs < 1 || !h_series || !h_lens || !job_begin || !job_end || !job_flags ||             \
+        !h_medoids || !h_centroid_offsets || !h_centroids || !h_rounds || !h_deltas)             \
+      return ODBA_ERR_INVALID_ARGUMENT;                                                          \
+    for (int j = 0; j < njobs; ++j)                                                              \
+      if (job_end[j] <= job_begin[j] || (j && job_begin[j] != job_end[j - 1]) ||                 \
+          (j == 0 && job_begin[0] != 0))                                                         \
+        return ODBA_ERR_INVALID_ARGUMENT;                                                        \
+    /* graphs cannot be captured on the legacy default stream: run on a private      */    \
+    /* stream ordered after the caller's                                              */    \
+    cudaStream_t caller = static_cast<cudaStream_t>(stream), own = nullptr;                      \
+    cudaEvent_t ready = nullptr;                                                                 \
+    check_cuda(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking), "job stream");            \
+    check_cuda(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "job event");           \
+    check_cuda(cudaEventRecord(ready, caller), "job event");                                     \
+    check_cuda(cudaStreamWaitEvent(own, ready, 0), "job event");                                 \
+    const int rc = run_jobs<T>(h_series, h_lens, job_begin, job_end, job_flags, njobs, norm,     \
+                               max_rounds > 0 ? max_rounds : 250, batched != 0, h_medoids,       \
+                               h_centroid_offsets, h_centroids, h_rounds, h_deltas, own);        \
+    check_cuda(cudaStreamSynchronize(own), "job stream");                                        \
+    cudaEventDestroy(ready);                                                                     \
+    cudaStreamDestroy(own);                                                                      \
+    return rc;                                                                                   \
+  }
+ODBA_JOBS_ENTRY(f32, float)
+ODBA_JOBS_ENTRY(f64, double)
+#undef ODBA_JOBS_ENTRY

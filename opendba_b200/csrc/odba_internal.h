@@ -27,6 +27,11 @@ int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *le
                     cudaStream_t stream);
 
 template <typename T>
+int pairlist_launch(const T *series, const uint64_t *offsets, const uint64_t *lens,
+                    const odba_pair_task *tasks, unsigned long long ntasks, uint64_t max_len,
+                    T *dists, void *workspace, size_t ws_bytes, cudaStream_t stream);
+
+template <typename T>
 int medoid_launch(const T *dists, const uint64_t *lens, int n, T *sos, int *medoid,
                   cudaStream_t stream);
 
@@ -41,6 +46,19 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
                      const uint64_t *lens, const uint64_t *h_lens, int n, int os, int oe, T *mean,
                      uint32_t *counts, double *delta, int32_t *triples, int64_t *triple_counts,
                      void *ws, size_t ws_bytes, cudaStream_t stream);
+
+template <typename T>
+size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int nmem,
+                                 const uint64_t *h_clen, const int *h_flags, int njobs);
+template <typename T>
+int dba_batch_launch(const T *centroids, const unsigned long long *coff, const int *clen,
+                     const int *jflags, const int *mbeg, const int *mend, int njobs, int max_clen,
+                     const T *series, const uint64_t *offsets, const uint64_t *lens,
+                     const int *mseries, const int *mjob, const int *order, int nmem,
+                     const uint64_t *h_mlens, const int *h_mjob, const uint64_t *h_clen,
+                     const int *h_flags, T *means, uint32_t *counts, double *deltas,
+                     int32_t *triples, int64_t *triple_counts, void *ws, size_t ws_bytes,
+                     cudaStream_t stream);
 
 void segment_params(int minseg, int *dw, int *spb, int *k_max);
 template <typename T>
