@@ -69,7 +69,9 @@ int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const u
  * dists[out & (2^62 - 1)]; bit 62 of `out` selects open start, bit 63 open end.
  * Tasks are taken in array order (put the largest m*n first).  The workspace
  * is odba_dtw_pairwise_workspace_bytes(elem_size, max_len) with max_len the
- * longest `first` series. */
+ * longest `first` series.  series may be NULL: offsets are then element
+ * addresses (device address / element size), so series in separate
+ * allocations can share one launch. */
 typedef struct odba_pair_task {
   uint32_t first;
   uint32_t second;
@@ -159,7 +161,8 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
  * the tail short); it does not change any result.  Outputs per job at the
  * job's centroid offset: means, counts; deltas[J] = max |centroid - mean|.
  * The h_* arrays are host copies that size the workspace.  Results equal one
- * odba_dba_round_* call per job, bit for bit. */
+ * odba_dba_round_* call per job, bit for bit.  series may be NULL, with
+ * offsets as element addresses (see odba_dtw_pairlist_*). */
 size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_lens,
                                       const int *h_member_job, int nmem,
                                       const uint64_t *h_centroid_lens, const int *h_job_flags,
@@ -270,6 +273,34 @@ int odba_dba_jobs_f64(const double *h_series, const uint64_t *h_lens, const int 
                       const int *job_end, const int *job_flags, int njobs, int norm,
                       int max_rounds, int batched, int *h_medoids, uint64_t *h_centroid_offsets,
                       double *h_centroids, int *h_rounds, double *h_deltas, void *stream);
+
+/* ---- serving loop with continuous batching -----------------------------------
+ * No reference counterpart.  A server owns a worker thread on one device that
+ * batches whatever requests are admitted: each iteration runs one pair-list
+ * launch (every admitted query's pairs, every job's medoid pairs) and one
+ * batched DBA round (every job in its round stage); requests that arrive
+ * meanwhile join the next iteration; requests are admitted in arrival order
+ * while the estimated device memory of all admitted work stays under
+ * hbm_budget_bytes (one request is always admitted).  Centroids added with
+ * odba_server_add_centroid stay resident.  A query aligns each of nreads reads
+ * (first series) to each listed centroid (second series) and returns nreads x
+ * ncentroids pair distances, row-major; a job is performDBA for one cluster
+ * (see odba_dba_jobs_*) and returns the centroid.  Results do not depend on
+ * what else was batched.  submit returns a request id (> 0) or -status; poll
+ * returns 0 running, 1 done, -status failed; wait blocks up to timeout_s;
+ * take copies the result out (capacity in elements) and forgets the request. */
+void *odba_server_create(int elem_size, size_t hbm_budget_bytes, int device);
+void odba_server_destroy(void *server);
+int odba_server_add_centroid(void *server, const void *h_centroid, uint64_t len);
+int64_t odba_server_submit_query(void *server, const void *h_reads, const uint64_t *h_read_lens,
+                                 int nreads, const int *centroid_ids, int ncentroids, int flags);
+int64_t odba_server_submit_job(void *server, const void *h_series, const uint64_t *h_lens, int n,
+                               int flags, int norm);
+int odba_server_poll(void *server, int64_t request);
+int odba_server_wait(void *server, int64_t request, double timeout_s);
+int odba_server_take(void *server, int64_t request, void *h_out, uint64_t capacity,
+                     uint64_t *out_len, int *medoid, int *rounds, double *latency_s);
+int odba_server_stats(void *server, uint64_t *iterations, uint64_t *cells, double *busy_s);
 
 #ifdef __cplusplus
 }

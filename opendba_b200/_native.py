@@ -64,6 +64,15 @@ SIGNATURES = {
     "odba_segment_host_f64": (I32, [P, P, I32, I32, I32, P, P]),
     "odba_dba_jobs_f32": (I32, [P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P]),
     "odba_dba_jobs_f64": (I32, [P, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P]),
+    "odba_server_create": (P, [I32, ctypes.c_size_t, I32]),
+    "odba_server_destroy": (None, [P]),
+    "odba_server_add_centroid": (I32, [P, P, U64]),
+    "odba_server_submit_query": (ctypes.c_int64, [P, P, P, I32, P, I32, I32]),
+    "odba_server_submit_job": (ctypes.c_int64, [P, P, P, I32, I32, I32]),
+    "odba_server_poll": (I32, [P, ctypes.c_int64]),
+    "odba_server_wait": (I32, [P, ctypes.c_int64, ctypes.c_double]),
+    "odba_server_take": (I32, [P, ctypes.c_int64, P, U64, P, P, P, P]),
+    "odba_server_stats": (I32, [P, P, P, P]),
     "odba_medoid_pass_host_f32": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
     "odba_medoid_pass_host_f64": (I32, [P, P, I32, I32, I32, I32, P, P, P, P, P]),
 }

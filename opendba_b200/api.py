@@ -280,3 +280,76 @@ def dba_jobs(jobs, flags=None, norm: int = 1, batched: bool = True, max_rounds: 
         out.append({"medoid": int(med[j]), "centroid": cent[o:o + L].copy(), "rounds": int(rounds[j]),
                     "delta": float(deltas[j])})
     return out
+
+
+class Server:
+    """Serving loop with continuous batching (odba_server_*)."""
+
+    def __init__(self, dtype=np.float32, hbm_budget_bytes: int = 8 << 30, device: int = 0):
+        self.dtype = np.dtype(dtype)
+        self._lib = _native.lib()
+        self._h = self._lib.odba_server_create(self.dtype.itemsize, int(hbm_budget_bytes), int(device))
+        self._keep = {}
+
+    def close(self):
+        if self._h:
+            self._lib.odba_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_centroid(self, centroid) -> int:
+        c = np.ascontiguousarray(centroid, dtype=self.dtype)
+        cid = self._lib.odba_server_add_centroid(self._h, c.ctypes.data, len(c))
+        if cid < 0:
+            raise _native.OdbaError(-cid, "add_centroid")
+        return cid
+
+    def submit_query(self, reads, centroid_ids, open_start=0, open_end=0) -> int:
+        flat, _, lens = pack_host(reads, self.dtype)
+        ids = np.ascontiguousarray(centroid_ids, dtype=np.int32)
+        rid = self._lib.odba_server_submit_query(self._h, flat.ctypes.data, lens.ctypes.data,
+                                                 len(lens), ids.ctypes.data, len(ids),
+                                                 int(open_start) | (int(open_end) << 1))
+        if rid < 0:
+            raise _native.OdbaError(-rid, "submit_query")
+        self._keep[rid] = ("q", len(lens) * len(ids))
+        return rid
+
+    def submit_job(self, series, open_start=0, open_end=0, norm=1) -> int:
+        flat, _, lens = pack_host(series, self.dtype)
+        rid = self._lib.odba_server_submit_job(self._h, flat.ctypes.data, lens.ctypes.data, len(lens),
+                                               int(open_start) | (int(open_end) << 1), int(norm))
+        if rid < 0:
+            raise _native.OdbaError(-rid, "submit_job")
+        self._keep[rid] = ("j", int(max(lens)))
+        return rid
+
+    def poll(self, rid) -> int:
+        return self._lib.odba_server_poll(self._h, rid)
+
+    def wait(self, rid, timeout_s=600.0) -> int:
+        return self._lib.odba_server_wait(self._h, rid, float(timeout_s))
+
+    def take(self, rid):
+        kind, cap = self._keep.pop(rid)
+        out = np.zeros(max(cap, 1), dtype=self.dtype)
+        n = ctypes.c_uint64(0)
+        med = ctypes.c_int(-1)
+        rounds = ctypes.c_int(0)
+        lat = ctypes.c_double(0)
+        rc = self._lib.odba_server_take(self._h, rid, out.ctypes.data, cap, ctypes.byref(n),
+                                        ctypes.byref(med), ctypes.byref(rounds), ctypes.byref(lat))
+        _native.check(rc)
+        return {"result": out[:n.value].copy(), "medoid": med.value, "rounds": rounds.value,
+                "latency_s": lat.value}
+
+    def stats(self):
+        it, cells, busy = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_double(0)
+        _native.check(self._lib.odba_server_stats(self._h, ctypes.byref(it), ctypes.byref(cells),
+                                                  ctypes.byref(busy)))
+        return {"iterations": it.value, "cells": cells.value, "busy_s": busy.value}

@@ -250,7 +250,7 @@ int odba_medoid_pass_host_f64(const double *h_series, const uint64_t *h_lens, in
 int odba_dtw_pairlist_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
                           const odba_pair_task *tasks, uint64_t ntasks, uint64_t max_len,
                           float *dists, void *workspace, size_t workspace_bytes, void *stream) {
-  if (ntasks && (!series || !offsets || !lens || !tasks || !dists || !workspace))
+  if (ntasks && (!offsets || !lens || !tasks || !dists || !workspace))
     return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer");
   if (max_len == 0 || max_len > (1ull << 31)) return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be in [1, 2^31]");
   if (int rc = require_sm100()) return rc;
@@ -261,7 +261,7 @@ int odba_dtw_pairlist_f32(const float *series, const uint64_t *offsets, const ui
 int odba_dtw_pairlist_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
                           const odba_pair_task *tasks, uint64_t ntasks, uint64_t max_len,
                           double *dists, void *workspace, size_t workspace_bytes, void *stream) {
-  if (ntasks && (!series || !offsets || !lens || !tasks || !dists || !workspace))
+  if (ntasks && (!offsets || !lens || !tasks || !dists || !workspace))
     return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer");
   if (max_len == 0 || max_len > (1ull << 31)) return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be in [1, 2^31]");
   if (int rc = require_sm100()) return rc;
@@ -321,7 +321,7 @@ size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_le
       const int *h_job_flags, T *means, uint32_t *counts, double *deltas, int32_t *path_triples, \
       int64_t *path_counts, void *workspace, size_t workspace_bytes, void *stream) {           \
     if (njobs < 1 || nmem < 1 || max_centroid_len < 1 || !centroids || !centroid_offsets ||    \
-        !centroid_lens || !job_flags || !job_member_begin || !job_member_end || !series ||     \
+        !centroid_lens || !job_flags || !job_member_begin || !job_member_end ||                \
         !offsets || !lens || !member_series || !member_job || !h_member_lens ||                \
         !h_member_job || !h_centroid_lens || !h_job_flags || !means || !counts || !deltas ||   \
         !workspace)                                                                            \
