@@ -206,6 +206,32 @@ def run_reference(args, world, rank):
     return 0
 
 
+def extra_results(which):
+    from opendba_b200 import workloads
+    out = {}
+    if which in ("batched", "all"):
+        out["batched_vs_plain"] = workloads.run_batched_vs_plain()
+    if which in ("serving", "all"):
+        out["serving"] = [workloads.run_serving(r) for r in (4.0, 64.0)]
+    return out
+
+
+def run_extra(args, world, rank, local):
+    """The batched and served forms against the plain per-job path (1 GPU)."""
+    import torch
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return 0
+    from opendba_b200 import build, _native
+    if not os.path.exists(_native.LIB_PATH):
+        build.build_library()
+    res = extra_results(args.workload)
+    line = {"metric": METRIC, "workload": args.workload, "n_gpus": 1, "dtype": "f32",
+            "data": "synthetic (seeded nanopore-like step signals)", **res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -217,10 +243,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--n-series", type=int, default=N_SERIES,
                     help="development only: fewer series than the benchmark configuration")
+    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "all"],
+                    help="medoid: the metric's configuration (default); batched: many DBA jobs, "
+                         "batched vs plain; serving: Poisson request stream, served vs plain; "
+                         "all: the medoid line with the other two added")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload in ("batched", "serving"):
+        return run_extra(args, world, rank, local)
 
     import torch
     torch.cuda.set_device(local)
@@ -340,6 +372,8 @@ def main():
         }
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline(synth.znorm_host(series_raw), args.cpu_secs)
+        if args.workload == "all" and world == 1:
+            line.update(extra_results("all"))
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

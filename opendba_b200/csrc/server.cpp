@@ -122,6 +122,20 @@ class Server {
   Server(size_t budget, int device) : budget_(budget), device_(device) {
     cudaSetDevice(device_);
     cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
+    // A private stream-ordered pool that keeps up to the HBM budget mapped:
+    // the device's default pool unmaps freed memory at every synchronisation,
+    // which would re-map the per-iteration workspaces on every iteration.
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device_;
+    if (cudaMemPoolCreate(&pool_, &props) == cudaSuccess) {
+      uint64_t keep = budget_;
+      cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+      cudaGetLastError();
+      pool_ = nullptr;
+    }
     worker_ = std::thread([this] { loop(); });
   }
   ~Server() {
@@ -132,7 +146,9 @@ class Server {
     cv_.notify_all();
     worker_.join();
     for (auto &kv : reqs_) release(*kv.second);
+    cudaStreamSynchronize(st_);
     for (auto &c : centroids_) cudaFree(c.d);
+    if (pool_) cudaMemPoolDestroy(pool_);
     cudaStreamDestroy(st_);
   }
 
@@ -254,15 +270,13 @@ class Server {
     return r->id;
   }
 
+  // Stream-ordered frees: no device-wide synchronisation per request.
   void release(Request<T> &r) {
-    cudaFree(r.d_series);
-    cudaFree(r.d_offs);
-    cudaFree(r.d_lens);
-    cudaFree(r.d_dists);
-    cudaFree(r.d_med);
-    cudaFree(r.d_sos);
-    cudaFree(r.d_mean);
-    cudaFree(r.d_sig);
+    for (void *p : {static_cast<void *>(r.d_series), static_cast<void *>(r.d_offs),
+                    static_cast<void *>(r.d_lens), static_cast<void *>(r.d_dists),
+                    static_cast<void *>(r.d_med), static_cast<void *>(r.d_sos),
+                    static_cast<void *>(r.d_mean), static_cast<void *>(r.d_sig)})
+      if (p) cudaFreeAsync(p, st_);
     r.d_series = nullptr;
     r.d_offs = r.d_lens = nullptr;
     r.d_dists = r.d_sos = nullptr;
@@ -280,6 +294,12 @@ class Server {
     done_cv_.notify_all();
   }
 
+  template <typename U>
+  cudaError_t dmalloc(U **p, size_t bytes) {
+    return pool_ ? cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool_, st_)
+                 : cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st_);
+  }
+
   // device copies of an admitted request
   bool upload(Request<T> &r) {
     const int n = int(r.lens.size());
@@ -289,9 +309,9 @@ class Server {
       offs[i] = acc;
       acc += r.lens[i];
     }
-    if (cudaMalloc(&r.d_series, (acc + 16) * sizeof(T)) != cudaSuccess ||
-        cudaMalloc(&r.d_offs, n * sizeof(uint64_t)) != cudaSuccess ||
-        cudaMalloc(&r.d_lens, n * sizeof(uint64_t)) != cudaSuccess)
+    if (dmalloc(&r.d_series, (acc + 16) * sizeof(T)) != cudaSuccess ||
+        dmalloc(&r.d_offs, n * sizeof(uint64_t)) != cudaSuccess ||
+        dmalloc(&r.d_lens, n * sizeof(uint64_t)) != cudaSuccess)
       return false;
     cudaMemcpyAsync(r.d_series, r.host.data(), acc * sizeof(T), cudaMemcpyHostToDevice, st_);
     cudaMemcpyAsync(r.d_offs, offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st_);
@@ -300,16 +320,16 @@ class Server {
     for (int i = 0; i < n; ++i)
       r.elem_addr[i] = reinterpret_cast<uint64_t>(r.d_series) / sizeof(T) + offs[i];
     if (!r.is_query) {
-      if (cudaMalloc(&r.d_mean, n * sizeof(double)) != cudaSuccess ||
-          cudaMalloc(&r.d_sig, n * sizeof(double)) != cudaSuccess)
+      if (dmalloc(&r.d_mean, n * sizeof(double)) != cudaSuccess ||
+          dmalloc(&r.d_sig, n * sizeof(double)) != cudaSuccess)
         return false;
       if (r.norm &&
           ServerOps<T>::znorm(r.d_series, r.d_offs, r.d_lens, n, r.d_mean, r.d_sig, st_) != ODBA_OK)
         return false;
       const size_t np = size_t(n) * (n - 1) / 2;
-      if (cudaMalloc(&r.d_dists, std::max<size_t>(np, 1) * sizeof(T)) != cudaSuccess ||
-          cudaMalloc(&r.d_sos, n * sizeof(T)) != cudaSuccess ||
-          cudaMalloc(&r.d_med, sizeof(int)) != cudaSuccess)
+      if (dmalloc(&r.d_dists, std::max<size_t>(np, 1) * sizeof(T)) != cudaSuccess ||
+          dmalloc(&r.d_sos, n * sizeof(T)) != cudaSuccess ||
+          dmalloc(&r.d_med, sizeof(int)) != cudaSuccess)
         return false;
       r.means.assign(n, 0.0);
       r.sigmas.assign(n, 1.0);
@@ -319,7 +339,7 @@ class Server {
       }
     } else {
       const size_t nd = r.lens.size() * r.centroid_ids.size();
-      if (cudaMalloc(&r.d_dists, std::max<size_t>(nd, 1) * sizeof(T)) != cudaSuccess) return false;
+      if (dmalloc(&r.d_dists, std::max<size_t>(nd, 1) * sizeof(T)) != cudaSuccess) return false;
     }
     return true;
   }
@@ -425,11 +445,11 @@ class Server {
       T *d_out = nullptr;
       void *ws = nullptr;
       const size_t wsb = odba_dtw_pairwise_workspace_bytes(sizeof(T), max_first);
-      bool ok = cudaMallocAsync(reinterpret_cast<void **>(&d_tasks), sorted.size() * sizeof(odba_pair_task), st_) == cudaSuccess &&
-                cudaMallocAsync(reinterpret_cast<void **>(&d_offs), offs.size() * 8, st_) == cudaSuccess &&
-                cudaMallocAsync(reinterpret_cast<void **>(&d_lens), lens.size() * 8, st_) == cudaSuccess &&
-                cudaMallocAsync(reinterpret_cast<void **>(&d_out), out_total * sizeof(T), st_) == cudaSuccess &&
-                cudaMallocAsync(&ws, wsb, st_) == cudaSuccess;
+      bool ok = dmalloc(&d_tasks, sorted.size() * sizeof(odba_pair_task)) == cudaSuccess &&
+                dmalloc(&d_offs, offs.size() * 8) == cudaSuccess &&
+                dmalloc(&d_lens, lens.size() * 8) == cudaSuccess &&
+                dmalloc(&d_out, out_total * sizeof(T)) == cudaSuccess &&
+                dmalloc(reinterpret_cast<char **>(&ws), wsb) == cudaSuccess;
       if (ok) {
         cudaMemcpyAsync(d_tasks, sorted.data(), sorted.size() * sizeof(odba_pair_task), cudaMemcpyHostToDevice, st_);
         cudaMemcpyAsync(d_offs, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st_);
@@ -537,7 +557,7 @@ class Server {
       o[i] = total;
       total += sz[i];
     }
-    if (cudaMallocAsync(reinterpret_cast<void **>(&blob), total, st_) != cudaSuccess) {
+    if (dmalloc(&blob, total) != cudaSuccess) {
       cudaGetLastError();
       for (auto &r : rj) finish(r, kFailed, ODBA_ERR_OUT_OF_MEMORY);
       return;
@@ -608,6 +628,7 @@ class Server {
   size_t budget_;
   int device_;
   cudaStream_t st_ = nullptr;
+  cudaMemPool_t pool_ = nullptr;
   std::mutex mu_, cmu_;
   std::condition_variable cv_, done_cv_;
   bool stop_ = false;

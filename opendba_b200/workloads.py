@@ -1,0 +1,170 @@
+"""Benchmark workloads beyond the medoid pass: many DBA jobs (batched vs the
+plain per-job path) and a Poisson request stream through the serving loop
+(continuous batching vs plain first-come-first-served).
+
+Seeded synthetic data stands in for nanopore reads: no public suite exists.
+Cells are full m x n DTW matrices (medoid pairs, query pairs, and member x
+centroid per DBA round), counted the same way for both paths.
+"""
+from __future__ import annotations
+
+import math
+import statistics
+import threading
+import time
+
+import numpy as np
+
+from . import api, synth
+
+
+def _logu_int(rng, lo, hi, size=None):
+    return np.exp(rng.uniform(math.log(lo), math.log(hi), size=size)).astype(np.int64)
+
+
+def _step(rng, L):
+    return synth.step_signal(rng, int(L), 90.0, 12.0, 10.0, 2.0).astype(np.float32)
+
+
+def make_jobs(n_jobs, count_lo, count_hi, len_lo, len_hi, seed):
+    """Independent averaging jobs: per job a log-uniform count of series with
+    log-uniform lengths."""
+    rng = np.random.default_rng(seed)
+    counts = _logu_int(rng, count_lo, count_hi + 1, n_jobs)
+    return [[_step(rng, L) for L in _logu_int(rng, len_lo, len_hi + 1, int(c))] for c in counts]
+
+
+def job_cells(job, rounds, centroid_len):
+    lens = np.array([len(s) for s in job], dtype=np.float64)
+    tot = lens.sum()
+    pair_cells = (tot * tot - (lens * lens).sum()) / 2.0
+    return pair_cells + rounds * tot * centroid_len
+
+
+def run_batched_vs_plain(n_jobs=48, count_lo=8, count_hi=96, len_lo=200, len_hi=4000,
+                         open_end=1, seed=0x0DBA0004):
+    """Many DBA jobs (open end, float32): batched vs plain; returns a dict."""
+    jobs = make_jobs(n_jobs, count_lo, count_hi, len_lo, len_hi, seed)
+    flags = [2 if open_end else 0] * len(jobs)
+    api.dba_jobs(jobs[:2], flags[:2], norm=1, batched=True)   # warm-up (module loading)
+    api.dba_jobs(jobs[:2], flags[:2], norm=1, batched=False)
+    t0 = time.perf_counter()
+    res_b = api.dba_jobs(jobs, flags, norm=1, batched=True)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res_p = api.dba_jobs(jobs, flags, norm=1, batched=False)
+    tp = time.perf_counter() - t0
+    same = all(a["medoid"] == b["medoid"] and a["rounds"] == b["rounds"] and
+               np.array_equal(a["centroid"].view(np.uint32), b["centroid"].view(np.uint32))
+               for a, b in zip(res_b, res_p))
+    cells = sum(job_cells(j, r["rounds"], len(r["centroid"])) for j, r in zip(jobs, res_b))
+    return {"workload": f"{len(jobs)} DBA jobs of {count_lo}-{count_hi} series (log-uniform), lengths "
+                        f"log-uniform [{len_lo},{len_hi}], open end, float32, z-normalised",
+            "cells": cells, "batched_s": tb, "plain_s": tp,
+            "batched_gcups": cells / tb / 1e9, "plain_gcups": cells / tp / 1e9,
+            "speedup": tp / tb, "identical_results": bool(same),
+            "rounds_mean": float(np.mean([r["rounds"] for r in res_b]))}
+
+
+def make_requests(n, seed, n_centroids=32, centroid_len=4000, query_frac=0.7,
+                  reads_max=64, read_lo=500, read_hi=50000, job_lo=16, job_hi=256,
+                  job_len=(500, 2000)):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for _ in range(n):
+        if rng.uniform() < query_frac:
+            k = int(_logu_int(rng, 1, reads_max + 1))
+            reads = [_step(rng, L) for L in _logu_int(rng, read_lo, read_hi + 1, k)]
+            reqs.append(("q", reads))
+        else:
+            k = int(_logu_int(rng, job_lo, job_hi + 1))
+            reqs.append(("j", [_step(rng, L) for L in rng.integers(job_len[0], job_len[1] + 1, k)]))
+    cents = [_step(rng, centroid_len) for _ in range(n_centroids)]
+    return reqs, cents
+
+
+def _request_cells(kind, data, cents, rounds=0, clen=0):
+    if kind == "q":
+        return float(sum(len(r) for r in data)) * float(sum(len(c) for c in cents))
+    return job_cells(data, rounds, clen)
+
+
+def run_serving(rate_hz, n_requests=60, seed=0x0DBA0005, budget=32 << 30, detail=False, **kw):
+    """Poisson arrivals through the server; returns latency percentiles and
+    throughput, plus the plain FCFS path on the same requests."""
+    reqs, cents = make_requests(n_requests, seed, **kw)
+    rng = np.random.default_rng(seed + 1)
+    gaps = rng.exponential(1.0 / rate_hz, size=len(reqs))
+    srv = api.Server(np.float32, hbm_budget_bytes=budget)
+    ids = [srv.add_centroid(c) for c in cents]
+    # warm-up
+    w = srv.submit_query([cents[0][:500]], ids[:2])
+    srv.wait(w, 300)
+    srv.take(w)
+    submitted = []
+    t_start = time.perf_counter()
+
+    def producer():
+        for (kind, data), g in zip(reqs, gaps):
+            time.sleep(g)
+            rid = srv.submit_query(data, ids) if kind == "q" else srv.submit_job(data)
+            submitted.append((rid, kind, data))
+
+    th = threading.Thread(target=producer)
+    th.start()
+    th.join()
+    lats, cells, rounds = [], 0.0, []
+    for rid, kind, data in submitted:
+        assert srv.wait(rid, 1200) == 1
+        r = srv.take(rid)
+        lats.append(r["latency_s"])
+        rounds.append(r["rounds"])
+        cells += _request_cells(kind, data, cents, r["rounds"], len(r["result"]) if kind == "j" else 0)
+    wall = time.perf_counter() - t_start
+    sstats = srv.stats()
+    srv.close()
+    # plain: the same requests one after another through the drop-in paths
+    t0 = time.perf_counter()
+    plain_lat, plain_dur, clock = [], [], 0.0
+    arrivals = np.cumsum(gaps)
+    for (kind, data), arr in zip(reqs, arrivals):
+        s0 = time.perf_counter()
+        if kind == "q":
+            ds = api.DeviceSeries.from_host(list(data) + cents)
+            n = len(data)
+            import torch
+            tasks = np.zeros(n * len(cents), dtype=[("first", "<u4"), ("second", "<u4"), ("out", "<u8")])
+            k = 0
+            for i in range(n):
+                for c in range(len(cents)):
+                    tasks[k] = (i, n + c, k)
+                    k += 1
+            d_tasks = torch.from_numpy(tasks.view(np.uint8)).cuda()
+            out = torch.empty(k, dtype=torch.float32, device="cuda")
+            wsz = api._native.lib().odba_dtw_pairwise_workspace_bytes(4, max(len(r) for r in data))
+            ws = torch.empty(wsz, dtype=torch.uint8, device="cuda")
+            api._native.call("odba_dtw_pairlist_f32", ds.data.data_ptr(), ds.offsets.data_ptr(),
+                             ds.lens.data_ptr(), d_tasks.data_ptr(), k, max(len(r) for r in data),
+                             out.data_ptr(), ws.data_ptr(), ws.numel(),
+                             torch.cuda.current_stream().cuda_stream)
+            out.cpu()
+        else:
+            api.dba_jobs([data], [0], norm=1, batched=False)
+        dur = time.perf_counter() - s0
+        plain_dur.append(dur)
+        clock = max(clock, arr) + dur
+        plain_lat.append(clock - arr)
+    plain_wall = time.perf_counter() - t0
+    pct = lambda v, p: float(np.percentile(np.array(v), p))  # noqa: E731
+    out = {"rate_hz": rate_hz, "requests": len(reqs), "cells": cells,
+            "served_wall_s": wall, "served_gcups": cells / wall / 1e9,
+            "p50_ms": 1e3 * pct(lats, 50), "p99_ms": 1e3 * pct(lats, 99),
+            "plain_busy_s": plain_wall, "plain_gcups": cells / plain_wall / 1e9,
+            "plain_p50_ms": 1e3 * pct(plain_lat, 50), "plain_p99_ms": 1e3 * pct(plain_lat, 99),
+            "server_iterations": sstats["iterations"], "server_busy_s": sstats["busy_s"]}
+    if detail:
+        out["requests_detail"] = [
+            {"kind": k, "n": len(d), "samples": int(sum(len(x) for x in d)), "rounds": rr,
+             "served_ms": 1e3 * l, "plain_ms": 1e3 * pd}
+            for (k, d), rr, l, pd in zip(reqs, rounds, lats, plain_dur)]
+    return out
