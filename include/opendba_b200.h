@@ -49,16 +49,63 @@ int odba_device_check(void);
  * Replaces the DTWDistance launch loop of approximateMedoidIndices
  * (dba.hpp:37-161, kernel dtw.hpp:39-259) for one device.  Series s is the
  * first (row) series of pair (s, j), as in the reference.  The workspace holds
- * a work counter and per-warp swath-edge buffers; its size depends only on the
- * element size and the longest series.  use_open_start / use_open_end have the
- * reference's meaning (openDBA.cu:72-104). */
+ * a work counter and swath-edge buffers.  odba_dtw_pairwise_workspace_bytes
+ * depends only on the element size and the longest series and fits every
+ * launch plan when there are at most as many pairs as resident warps;
+ * odba_dtw_pairwise_workspace_bytes_n is the tighter size of the plan chosen
+ * by default for n series (few long series: per-pair edge buffers instead of
+ * per-warp ones).  A smaller workspace restricts the plans to those that fit.
+ * use_open_start / use_open_end have the reference's meaning
+ * (openDBA.cu:72-104).  If a swath hand-off wait of the pipelined plan runs
+ * out (it never does in a healthy launch), the pairs it touched read NaN and
+ * the word at byte 8 of the workspace is non-zero. */
 size_t odba_dtw_pairwise_workspace_bytes(int elem_size, uint64_t max_len);
+size_t odba_dtw_pairwise_workspace_bytes_n(int elem_size, int n, uint64_t max_len);
 int odba_dtw_pairwise_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
                           int n, uint64_t max_len, int use_open_start, int use_open_end,
                           float *dists, void *workspace, size_t workspace_bytes, void *stream);
 int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
                           int n, uint64_t max_len, int use_open_start, int use_open_end,
                           double *dists, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- launch plans of the pair kernels, and their autotuner -------------------
+ * No reference counterpart (the reference has one launch shape).  Every plan
+ * gives the same distances bit for bit:
+ *   ODBA_PLAN_WHOLE_PAIR             one warp per pair, 1024-column swaths
+ *                                    (512 for double), persistent work queue;
+ *   ODBA_PLAN_WHOLE_PAIR_HALF_SWATH  the same with half-width swaths;
+ *   ODBA_PLAN_SWATH_PIPELINE         many warps per pair: swaths of one pair
+ *                                    run on different warps, each waiting
+ *                                    (bounded) on the previous swath's edge.
+ * The plan is chosen per key (element size, len_bucket = floor(log2 max_len),
+ * count_bucket = floor(log2 pairs)): a plan pinned with odba_tune_set; else,
+ * in tuning mode (odba_tune_mode(1)), each eligible plan not yet measured for
+ * the key, launch by launch; else the fastest measured plan; else a rule of
+ * thumb.  odba_tune_query reports the plan the next launch would use and the
+ * measured rates (pairs * max_len^2 per second, ODBA_PLAN_COUNT doubles,
+ * index = plan).  odba_tune_flush waits for pending measurements;
+ * odba_tune_save / odba_tune_load write and read the table as text. */
+enum {
+  ODBA_PLAN_AUTO = 0,
+  ODBA_PLAN_WHOLE_PAIR = 1,
+  ODBA_PLAN_WHOLE_PAIR_HALF_SWATH = 2,
+  ODBA_PLAN_SWATH_PIPELINE = 3,
+  ODBA_PLAN_COUNT = 4
+};
+int odba_tune_set(int elem_size, int len_bucket, int count_bucket, int plan);
+int odba_tune_query(int elem_size, uint64_t max_len, uint64_t npairs, size_t workspace_bytes,
+                    int *plan, double *rates);
+void odba_tune_mode(int on);
+int odba_tune_flush(void);
+int odba_tune_save(const char *path);
+int odba_tune_load(const char *path);
+
+/* ---- self-test of the bounded device wait --------------------------------------
+ * No reference counterpart.  One warp runs the swath pipeline's wait on a
+ * progress word that nothing publishes, with the given limit (at most 10 s);
+ * returns ODBA_ERR_TIMEOUT when the wait ran out and raised the error word,
+ * as it must. */
+int odba_selftest_wait_timeout(uint64_t limit_ns, void *stream);
 
 /* ---- DTW distances of an arbitrary pair list (batched jobs, queries) ----------
  * No single reference counterpart: the batched form of the medoid launches of

@@ -79,7 +79,7 @@ int medoid_pass_host(const T *h_series, const uint64_t *h_lens, int n, int os, i
     if (h_lens[i] > max_len) max_len = h_lens[i];
   }
   const size_t npairs = size_t(n) * (n - 1) / 2;
-  const size_t ws_bytes = pairwise_workspace_bytes<T>(max_len);
+  const size_t ws_bytes = pairwise_workspace_bytes_n<T>(npairs, max_len);
   // one device allocation: series | offsets | lens | dists | sos | means | sigmas | medoid | workspace
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_series = up((total + 16) * sizeof(T)), b_meta = up(n * sizeof(uint64_t)),
@@ -98,6 +98,7 @@ int medoid_pass_host(const T *h_series, const uint64_t *h_lens, int n, int os, i
   int *d_medoid = reinterpret_cast<int *>(base + b_series + 2 * b_meta + b_d + b_sos + 2 * b_mv);
   void *d_ws = base + b_series + 2 * b_meta + b_d + b_sos + 2 * b_mv + b_med;
   int rc = ODBA_OK;
+  unsigned wait_err = 0;
   auto run = [&]() -> int {
     ODBA_CUDA(cudaMemcpyAsync(d_series, h_series, total * sizeof(T), cudaMemcpyHostToDevice, stream),
               "series upload");
@@ -125,7 +126,12 @@ int medoid_pass_host(const T *h_series, const uint64_t *h_lens, int n, int os, i
     if (norm && h_sigmas)
       ODBA_CUDA(cudaMemcpyAsync(h_sigmas, d_sigmas, n * sizeof(double), cudaMemcpyDeviceToHost, stream),
                 "sigmas download");
+    if (n >= 2)
+      ODBA_CUDA(cudaMemcpyAsync(&wait_err, static_cast<char *>(d_ws) + 8, sizeof(unsigned),
+                                cudaMemcpyDeviceToHost, stream),
+                "error word download");
     ODBA_CUDA(cudaStreamSynchronize(stream), "medoid pass");
+    if (wait_err) return fail(ODBA_ERR_TIMEOUT, "a swath hand-off wait ran out in the pair kernel");
     return ODBA_OK;
   };
   rc = run();
@@ -185,6 +191,39 @@ int odba_device_check(void) { return require_sm100(); }
 size_t odba_dtw_pairwise_workspace_bytes(int elem_size, uint64_t max_len) {
   if (elem_size == 8) return pairwise_workspace_bytes<double>(max_len);
   return pairwise_workspace_bytes<float>(max_len);
+}
+
+size_t odba_dtw_pairwise_workspace_bytes_n(int elem_size, int n, uint64_t max_len) {
+  const unsigned long long npairs = n > 1 ? (unsigned long long)n * (n - 1) / 2 : 0;
+  if (elem_size == 8) return pairwise_workspace_bytes_n<double>(npairs, max_len);
+  return pairwise_workspace_bytes_n<float>(npairs, max_len);
+}
+
+int odba_tune_set(int elem_size, int len_bucket, int count_bucket, int plan) {
+  return tune_set(elem_size, len_bucket, count_bucket, plan);
+}
+
+int odba_tune_query(int elem_size, uint64_t max_len, uint64_t npairs, size_t workspace_bytes,
+                    int *plan, double *rates) {
+  return tune_query(elem_size, max_len, npairs, workspace_bytes, plan, rates);
+}
+
+void odba_tune_mode(int on) { tune_mode(on); }
+
+int odba_tune_flush(void) { return tune_flush(); }
+
+int odba_tune_save(const char *path) {
+  if (!path) return fail(ODBA_ERR_INVALID_ARGUMENT, "null path");
+  return tune_save(path);
+}
+
+int odba_tune_load(const char *path) {
+  if (!path) return fail(ODBA_ERR_INVALID_ARGUMENT, "null path");
+  return tune_load(path);
+}
+
+int odba_selftest_wait_timeout(uint64_t limit_ns, void *stream) {
+  return gate_selftest(limit_ns, static_cast<cudaStream_t>(stream));
 }
 
 int odba_dtw_pairwise_f32(const float *series, const uint64_t *offsets, const uint64_t *lens, int n,

@@ -131,11 +131,22 @@ struct Pair2<double> {
   using V = double2;
 };
 
+// Hand-off of swath-edge rows between warps.  NoGate: the edge buffer is the
+// warp's own (written by the same warp's previous swath), nothing to wait for.
+// A gate with kActive set makes lane 0 call wait_in(k) before it reads edge
+// rows [0, k) and lane 31 call publish(k) once rows [0, k) are stored.
+struct NoGate {
+  static constexpr bool kActive = false;
+  __device__ __forceinline__ void wait_in(int) {}
+  __device__ __forceinline__ void publish(int) {}
+};
+constexpr int kPublishSteps = 64;  // lane 31 publishes every 64 steps (128 rows)
+
 // Sweeps one swath.  On return col[] holds, per lane, the costs of the last
 // row m-1 at the lane's columns.  Swath-edge buffers are indexed by r - r0,
 // two rows per 8/16-byte access.
-template <typename T, int R>
-__device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R]) {
+template <typename T, int R, typename Gate = NoGate>
+__device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R], Gate gate = Gate()) {
   using V2 = typename Pair2<T>::V;
   const int lane = threadIdx.x & 31;
   const int m = job.m;
@@ -173,6 +184,7 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R])
     xa = job.x[ia];
     xb = job.x[ib];
     if (has_in) {
+      if (Gate::kActive) gate.wait_in(rows > 0 ? kb + 1 : 0);
       ea = job.edge_in[ka];
       eb = job.edge_in[kb];
     } else {
@@ -232,10 +244,12 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R])
         v.x = a_last;
         v.y = col[R - 1];
         *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
+        if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1) gate.publish(2 * (t - 31) + 2);
       }
     }
   }
   for (; t < total; ++t) masked_step(t);
+  if (Gate::kActive && lane31 && has_out) gate.publish(rows);
 }
 
 // Reads the cost at absolute column cabs (which must lie in this swath) from

@@ -27,6 +27,20 @@ int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *le
                     cudaStream_t stream);
 
 template <typename T>
+size_t pairwise_workspace_bytes_n(unsigned long long npairs, uint64_t max_len);
+
+// Autotuner of the pair kernels' launch plan (ODBA_PLAN_*).
+int tune_set(int elem_size, int len_bucket, int count_bucket, int plan);
+int tune_query(int elem_size, uint64_t max_len, unsigned long long npairs, size_t ws_bytes, int *plan,
+               double *rates);
+void tune_mode(int on);
+int tune_flush();
+int tune_save(const char *path);
+int tune_load(const char *path);
+// Runs the swath pipeline's bounded wait on a word nothing publishes.
+int gate_selftest(unsigned long long limit_ns, cudaStream_t stream);
+
+template <typename T>
 int pairlist_launch(const T *series, const uint64_t *offsets, const uint64_t *lens,
                     const odba_pair_task *tasks, unsigned long long ntasks, uint64_t max_len,
                     T *dists, void *workspace, size_t ws_bytes, cudaStream_t stream);

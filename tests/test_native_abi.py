@@ -52,3 +52,26 @@ def test_status_strings_without_gpu(native):
     assert native.odba_abi_version() == 1
     assert native.odba_status_string(0) == b"ok"
     assert native.odba_status_string(4) == b"workspace too small"
+
+
+def test_tuning_table_set_save_load_without_gpu(native, tmp_path):
+    from opendba_b200 import _native
+    lib = _native.lib()
+    path = str(tmp_path / "tune.txt").encode()
+    assert lib.odba_tune_set(4, 21, 6, 3) == 0
+    assert lib.odba_tune_set(8, 12, 20, 1) == 0
+    assert lib.odba_tune_set(3, 12, 20, 1) == 1          # bad element size
+    assert lib.odba_tune_set(4, 12, 20, 9) == 1          # bad plan
+    assert lib.odba_tune_save(path) == 0
+    lines = [l.split() for l in open(path) if not l.startswith("#")]
+    assert ["4", "21", "6", "3"] == lines[0][:4] and ["8", "12", "20", "1"] == lines[1][:4]
+    assert lib.odba_tune_set(4, 21, 6, 0) == 0 and lib.odba_tune_set(8, 12, 20, 0) == 0
+    assert lib.odba_tune_load(path) == 0
+    assert lib.odba_tune_save(path) == 0
+    again = [l.split() for l in open(path) if not l.startswith("#")]
+    assert again == lines
+    bad = tmp_path / "bad.txt"
+    bad.write_text("4 21 6\n")
+    assert lib.odba_tune_load(str(bad).encode()) == 7
+    lib.odba_tune_set(4, 21, 6, 0)
+    lib.odba_tune_set(8, 12, 20, 0)
