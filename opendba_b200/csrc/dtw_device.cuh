@@ -43,13 +43,16 @@ struct Num<float> {
     return r;
   }
 };
+// Costs are never NaN and never -0 (they start at +0 or d*d and only grow), so
+// a compare-and-select minimum gives the same bits as fmin without fmin's NaN
+// handling, which costs several extra instructions per call in double.
 template <>
 struct Num<double> {
   static __device__ __forceinline__ double big() { return DBL_MAX; }
   static __device__ __forceinline__ double cell(double d, double m) { return __fma_rn(d, d, m); }
-  static __device__ __forceinline__ double min2(double a, double b) { return fmin(a, b); }
+  static __device__ __forceinline__ double min2(double a, double b) { return b < a ? b : a; }
   static __device__ __forceinline__ double min3(double a, double b, double c) {
-    return fmin(fmin(a, b), c);
+    return min2(min2(a, b), c);
   }
 };
 
@@ -66,7 +69,26 @@ struct SwathJob {
   bool open_end;
   bool free_diag0;    // column c0 is a reference swath-left column (c0 % 1024 == 0, c0 > 0)
   T corner_init;      // diagonal input of lane 0 at its first row
+  T *stage;           // this warp's kStageElems elements of shared memory
 };
+
+// Staging of lane 0's row inputs: in the steady state the whole warp copies
+// the x values and left-edge costs of the next 64 rows (one chunk, 32 steps)
+// into shared memory with cp.async, one chunk ahead, so that lane 0 reads
+// them from shared memory instead of waiting on L2.  Two slots of
+// [x[64] | edge[64]] per warp.
+constexpr int kChunkRows = 64;
+constexpr int kStageElems = 2 * 2 * kChunkRows;
+
+__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, int bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // One cell: the open-end top-row rule when TOP (the right move is free,
 // dtw.hpp:196-200; at a reference swath-left column the diagonal is free too,
@@ -212,6 +234,45 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
     }
   };
 
+  // chunk c of lane 0's rows (k = ra - r0 in [64c, 64c + 64)) into slot c % 2;
+  // each lane copies rows 2*lane, 2*lane + 1 of the chunk (clamped like fetch)
+  auto issue_chunk = [&](int c) {
+    T *slot = job.stage + (c & 1) * (2 * kChunkRows);
+    const int k = c * kChunkRows + 2 * lane;
+    const int ia = r0 + k < last_x ? r0 + k : last_x;
+    const int ib = r0 + k + 1 < last_x ? r0 + k + 1 : last_x;
+    cp_async_elem(slot + 2 * lane, job.x + ia, sizeof(T));
+    cp_async_elem(slot + 2 * lane + 1, job.x + ib, sizeof(T));
+    if (has_in) {
+      const int ka = k < last_e ? k : last_e, kb = k + 1 < last_e ? k + 1 : last_e;
+      cp_async_elem(slot + kChunkRows + 2 * lane, job.edge_in + ka, sizeof(T));
+      cp_async_elem(slot + kChunkRows + 2 * lane + 1, job.edge_in + kb, sizeof(T));
+    }
+    cp_async_commit();
+  };
+  // edge rows of chunk c must be published before any lane copies them
+  auto gate_chunk = [&](int c) {
+    if (Gate::kActive && has_in && lane0) {
+      const int need = (c + 1) * kChunkRows;
+      gate.wait_in(rows < need ? rows : need);
+    }
+  };
+  // lane 0's staged inputs of step u
+  auto staged = [&](int u, T &xa, T &xb, T &ea, T &eb) {
+    const T *slot = job.stage + ((u >> 5) & 1) * (2 * kChunkRows);
+    const int i = 2 * (u & 31);
+    const V2 xv = *reinterpret_cast<const V2 *>(slot + i);
+    xa = xv.x;
+    xb = xv.y;
+    if (has_in) {
+      const V2 ev = *reinterpret_cast<const V2 *>(slot + kChunkRows + i);
+      ea = ev.x;
+      eb = ev.y;
+    } else {
+      ea = eb = Num<T>::big();
+    }
+  };
+
   // steady state: rows a, b of every lane in [r0, m-2]
   int steady_end = (rows - 1) / 2;  // first step at which lane 0's row b reaches m-1
   if (steady_end < 31) steady_end = 31;
@@ -219,19 +280,36 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
   int t = 0;
   for (; t < fill_end; ++t) masked_step(t);
   if (t < steady_end) {
+    // chunks of steps t and t + 1 (the same chunk or two consecutive ones)
+    const int cfirst = t >> 5;
+    gate_chunk(cfirst + 1);
+    __syncwarp();
+    issue_chunk(cfirst);
+    issue_chunk(cfirst + 1);
+    cp_async_wait_all();
+    __syncwarp();
     T pxa = T(0), pxb = T(0), pea = T(0), peb = T(0);
-    if (lane0) fetch(t, pxa, pxb, pea, peb);
+    if (lane0) staged(t, pxa, pxb, pea, peb);
     for (; t < steady_end; ++t) {
       T xa = __shfl_up_sync(kFull, xa_cur, 1);
       T xb = __shfl_up_sync(kFull, xb_cur, 1);
       T la = __shfl_up_sync(kFull, a_last, 1);
       T lb = __shfl_up_sync(kFull, col[R - 1], 1);
+      if (((t + 1) & 31) == 0) {
+        // step t + 1 opens chunk c1 (already copied); copy chunk c1 + 1 into
+        // the slot of chunk c1 - 1, whose last read was the previous step's
+        const int c1 = (t + 1) >> 5;
+        cp_async_wait_all();
+        gate_chunk(c1 + 1);
+        __syncwarp();
+        issue_chunk(c1 + 1);
+      }
       if (lane0) {
         xa = pxa;
         xb = pxb;
         la = pea;
         lb = peb;
-        fetch(t + 1, pxa, pxb, pea, peb);
+        staged(t + 1, pxa, pxb, pea, peb);
       }
       const T diag = dg;
       dg = lb;
@@ -247,6 +325,9 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
         if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1) gate.publish(2 * (t - 31) + 2);
       }
     }
+    // the next swath reuses the slots: no copy may still be in flight
+    cp_async_wait_all();
+    __syncwarp();
   }
   for (; t < total; ++t) masked_step(t);
   if (Gate::kActive && lane31 && has_out) gate.publish(rows);

@@ -128,6 +128,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
 template <typename T, int RF, int RQ>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     pairwise_kernel(PairwiseArgs<T> a) {
+  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
   const int lane = threadIdx.x & 31;
   const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   T *e0 = a.edges + slot * 2 * a.edge_stride;
@@ -141,6 +142,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     int s, j;
     pair_of(p, a.n, s, j);
     SwathJob<T> job;
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     job.x = a.series + a.offsets[s];
     job.m = int(a.lens[s]);
     job.y = a.series + a.offsets[j];
@@ -324,6 +326,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     pairlist_kernel(const T *series, const uint64_t *offsets, const uint64_t *lens,
                     const odba_pair_task *tasks, unsigned long long ntasks, T *dists,
                     unsigned long long *counter, T *edges, unsigned long long edge_stride) {
+  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
   const int lane = threadIdx.x & 31;
   const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   T *e0 = edges + slot * 2 * edge_stride;
@@ -337,6 +340,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     const int os = int((task.out >> 62) & 1ull), oe = int((task.out >> 63) & 1ull);
     const unsigned long long out = task.out & ((1ull << 62) - 1);
     SwathJob<T> job;
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     job.x = series + offsets[task.first];
     job.m = int(lens[task.first]);
     job.y = series + offsets[task.second];
@@ -482,6 +486,7 @@ template <typename T, int RF, int RQ>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     swathpipe_kernel(PipeArgs<T> a) {
   constexpr int W = 32 * RF;
+  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
   const int lane = threadIdx.x & 31;
   const unsigned long long ntasks = a.npairs * a.max_swaths;
   for (;;) {
@@ -507,6 +512,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
       out = (unsigned long long)p;
     }
     SwathJob<T> job;
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     job.x = a.series + a.offsets[s];
     job.m = int(a.lens[s]);
     job.y = a.series + a.offsets[j];
