@@ -13,9 +13,12 @@ same metric through the host-buffer C entry point odba_medoid_pass_host_f32
 (pinned host series in, distances/medoid/means/sigmas out, z-normalisation on
 the device), copies inside the timed region.
 
-Multi-GPU (torchrun): every rank runs its own medoid pass on its own seeded
-data set (pairs are independent; no data-path collective), so the work per GPU
-is fixed ("weak" scaling); the step time is the max over ranks.
+Multi-GPU (torchrun): one medoid pass over all ranks ("strong" scaling, the
+job is fixed): every rank holds the same series, computes a contiguous range
+of the pair triangle holding ~1/N of the DTW cells
+(odba_dtw_pairwise_range_f32), the ranges are exchanged with one NCCL
+all-gather of the distance triangle (8 MB), and every rank takes the medoid
+of the full triangle.  The step time is the max over ranks.
 
 ``--impl reference`` times the reference's DTW recurrence restated in C
 (oracle/, OpenMP on all host cores, the reference itself has no CPU
@@ -213,6 +216,8 @@ def extra_results(which):
         out["batched_vs_plain"] = workloads.run_batched_vs_plain()
     if which in ("serving", "all"):
         out["serving"] = [workloads.run_serving(r) for r in (4.0, 64.0)]
+    if which == "long":
+        out["long_pairs"] = workloads.run_long()
     return out
 
 
@@ -225,9 +230,11 @@ def run_extra(args, world, rank, local):
     from opendba_b200 import build, _native
     if not os.path.exists(_native.LIB_PATH):
         build.build_library()
-    res = extra_results(args.workload)
+    with ClockSampler(local) as clk:
+        res = extra_results(args.workload)
     line = {"metric": METRIC, "workload": args.workload, "n_gpus": 1, "dtype": "f32",
-            "data": "synthetic (seeded nanopore-like step signals)", **res}
+            "data": "synthetic (seeded nanopore-like step signals)", **res,
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -243,15 +250,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--n-series", type=int, default=N_SERIES,
                     help="development only: fewer series than the benchmark configuration")
-    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "all"],
+    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "long", "all"],
                     help="medoid: the metric's configuration (default); batched: many DBA jobs, "
                          "batched vs plain; serving: Poisson request stream, served vs plain; "
-                         "all: the medoid line with the other two added")
+                         "long: 16 series of 1M-4M samples, segmentation then all-vs-all f32 and "
+                         "f64 (several minutes); all: the medoid line with batched and serving added")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
-    if args.workload in ("batched", "serving"):
+    if args.workload in ("batched", "serving", "long"):
         return run_extra(args, world, rank, local)
 
     import torch
@@ -265,7 +273,7 @@ def main():
     from opendba_b200 import api, build, _native
     if not os.path.exists(_native.LIB_PATH):
         build.build_library()
-    series_raw, synth = workload(rank, args.n_series)
+    series_raw, synth = workload(0, args.n_series)  # one job shared by all ranks
     lens = [len(s) for s in series_raw]
     cells = cells_of(lens)
     stream = torch.cuda.current_stream()
@@ -277,13 +285,23 @@ def main():
     out = torch.empty(len(lens) * (len(lens) - 1) // 2, dtype=torch.float32, device=device)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MiB > L2
 
+    from opendba_b200 import sharding
+    ranges = sharding.shard_ranges(lens, world)
+    rb, re_ = ranges[rank]
+
     def step(evk=None):
         if evk is not None:
             evk[0].record(stream)
-        api.pairwise(ds, 0, 0, out=out, workspace=ws, stream=stream)
+        if world == 1:
+            api.pairwise(ds, 0, 0, out=out, workspace=ws, stream=stream)
+        else:
+            _native.call("odba_dtw_pairwise_range_f32", ds.data.data_ptr(), ds.offsets.data_ptr(),
+                         ds.lens.data_ptr(), ds.n, ds.max_len, 0, 0, rb, re_, out.data_ptr(),
+                         ws.data_ptr(), ws.numel(), stream.cuda_stream)
         if evk is not None:
             evk[1].record(stream)
-        return api.medoid(out, ds, stream=stream)
+        full = out if world == 1 else sharding.gather_triangle(out, ranges, rank, world)
+        return api.medoid(full, ds, stream=stream)
 
     for _ in range(args.warmup):
         step()
@@ -307,7 +325,7 @@ def main():
     barrier(world)
     ms = max_over_ranks(statistics.mean(step_ms), world, device)
     kms = max_over_ranks(statistics.mean(kern_ms), world, device)
-    value = world * cells / (ms * 1e-3) / 1e9
+    value = cells / (ms * 1e-3) / 1e9
 
     # end to end through the host-buffer C entry point (pinned host input)
     flat, _, hl = api.pack_host(series_raw)
@@ -316,23 +334,37 @@ def main():
     npairs = len(lens) * (len(lens) - 1) // 2
     dists_h = torch.empty(npairs, dtype=torch.float32).pin_memory().numpy()
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
-    api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)  # warm-up
+    dists_pin = torch.from_numpy(dists_h)
+
+    def e2e_step():
+        if world == 1:
+            return api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)[1]
+        # host series in (pinned), z-norm, this rank's range, all-gather, medoid, distances out
+        ds.data[: pinned.numel()].copy_(pinned, non_blocking=True)
+        api.znorm_(ds)
+        full, med = sharding.medoid_pass_sharded(ds, lens, rank, world, workspace=ws, stream=stream)
+        dists_pin.copy_(full, non_blocking=True)
+        torch.cuda.synchronize()
+        return med
+
+    e2e_step()  # warm-up
     barrier(world)
     e2e_s, med_e2e = [], None
     for _ in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, med_e2e, _, _ = api.medoid_pass_host(None, 0, 0, 1, flat=flat_p, lens=hl, dists_out=dists_h)
+        med_e2e = e2e_step()
         e2e_s.append(time.perf_counter() - t0)
     e2e_sec = max_over_ranks(statistics.mean(e2e_s), world, device) if e2e_s else float("nan")
-    e2e_value = world * cells / e2e_sec / 1e9
+    e2e_value = cells / e2e_sec / 1e9
     h2d = flat.nbytes + 2 * 8 * len(lens)
     d2h = npairs * 4 + 4 + 2 * 8 * len(lens)
 
     f_mhz = clocks["sm_mhz"] or SM_MAX_MHZ
     peak = SMS * FP32_LANES * f_mhz * 1e6 / OPS_PER_CELL / 1e9
     peak_max = SMS * FP32_LANES * SM_MAX_MHZ * 1e6 / OPS_PER_CELL / 1e9
-    achieved = cells / (kms * 1e-3) / 1e9
+    # the kernel of one rank processes its range: ~cells / world (balanced to 1%)
+    achieved = cells / world / (kms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "pairwise_dtw_traffic.json")
     if os.path.exists(tpath):
@@ -349,12 +381,14 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded nanopore-like step signals)",
             "config": {"workload": f"medoid all-vs-all: {args.n_series} series, lengths U[{LEN_LO},{LEN_HI}], "
                                    "global DTW, float32, z-normalised",
-                       "series": args.n_series, "pairs": npairs, "cells_per_gpu": cells,
-                       "len_range": [LEN_LO, LEN_HI], "mode": "global", "parallelism": f"pairs dp{world}",
+                       "series": args.n_series, "pairs": npairs, "cells": cells,
+                       "cells_per_gpu": cells / world, "len_range": [LEN_LO, LEN_HI], "mode": "global",
+                       "parallelism": ("pairs dp1" if world == 1 else
+                                       f"cell-balanced pair ranges x{world} + NCCL all-gather of the triangle"),
                        "l2": "256 MiB buffer written between timed steps"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "GCUPS",
                          "frac": achieved / peak, "traffic": traffic,
@@ -365,7 +399,9 @@ def main():
                          "hbm_peak_gbs_measured": hbm_gbs},
             "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "seconds_per_step": e2e_sec,
-                    "api": "odba_medoid_pass_host_f32 (z-norm + pairwise + medoid, pinned host buffers)"},
+                    "api": ("odba_medoid_pass_host_f32 (z-norm + pairwise + medoid, pinned host buffers)"
+                            if world == 1 else "pinned host series -> z-norm -> pair range -> all-gather "
+                            "-> medoid -> distances to pinned host, on every rank")},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
             "medoid": medoid_idx, "medoid_e2e": med_e2e,

@@ -68,6 +68,22 @@ int odba_dtw_pairwise_f64(const double *series, const uint64_t *offsets, const u
                           int n, uint64_t max_len, int use_open_start, int use_open_end,
                           double *dists, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- a range of the all-vs-all pairs (one device's share) -------------------
+ * Replaces one device's part of approximateMedoidIndices' launch loop, which
+ * deals the rows of the pair triangle to the devices in turn (dba.hpp:67-161).
+ * Computes pairs p in [pair_begin, pair_end) of the upper triangle (reference
+ * order, clustering.cuh:4-6) into dists[p] of a full-size triangle buffer;
+ * other entries are not touched.  Same workspace rules as
+ * odba_dtw_pairwise_*, with the pairs of the range in place of n(n-1)/2. */
+int odba_dtw_pairwise_range_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                                int n, uint64_t max_len, int use_open_start, int use_open_end,
+                                uint64_t pair_begin, uint64_t pair_end, float *dists,
+                                void *workspace, size_t workspace_bytes, void *stream);
+int odba_dtw_pairwise_range_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                                int n, uint64_t max_len, int use_open_start, int use_open_end,
+                                uint64_t pair_begin, uint64_t pair_end, double *dists,
+                                void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- launch plans of the pair kernels, and their autotuner -------------------
  * No reference counterpart (the reference has one launch shape).  Every plan
  * gives the same distances bit for bit:

@@ -32,6 +32,8 @@ SIGNATURES = {
     "odba_device_check": (I32, []),
     "odba_dtw_pairwise_workspace_bytes": (ctypes.c_size_t, [I32, U64]),
     "odba_dtw_pairwise_workspace_bytes_n": (ctypes.c_size_t, [I32, I32, U64]),
+    "odba_dtw_pairwise_range_f32": (I32, [P, P, P, I32, U64, I32, I32, U64, U64, P, P, ctypes.c_size_t, P]),
+    "odba_dtw_pairwise_range_f64": (I32, [P, P, P, I32, U64, I32, I32, U64, U64, P, P, ctypes.c_size_t, P]),
     "odba_tune_set": (I32, [I32, I32, I32, I32]),
     "odba_tune_query": (I32, [I32, U64, U64, ctypes.c_size_t, P, P]),
     "odba_tune_mode": (None, [I32]),

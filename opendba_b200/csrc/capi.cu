@@ -64,6 +64,22 @@ int pairwise_checked(const T *series, const uint64_t *offsets, const uint64_t *l
 }
 
 template <typename T>
+int pairwise_range_checked(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                           uint64_t max_len, int os, int oe, uint64_t pbeg, uint64_t pend, T *dists,
+                           void *ws, size_t ws_bytes, void *stream) {
+  const unsigned long long npairs = n > 1 ? (unsigned long long)n * (n - 1) / 2 : 0;
+  if (pbeg > pend || pend > npairs)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "pair range outside the upper triangle");
+  if (n < 0 || (pend > pbeg && (!series || !offsets || !lens || !dists || !ws)))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or negative series count");
+  if (max_len == 0 || max_len > (1ull << 31))
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be in [1, 2^31]");
+  if (int rc = require_sm100()) return rc;
+  return pairwise_range_launch<T>(series, offsets, lens, n, max_len, os ? 1 : 0, oe ? 1 : 0, pbeg,
+                                  pend, dists, ws, ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
+template <typename T>
 int medoid_pass_host(const T *h_series, const uint64_t *h_lens, int n, int os, int oe, int norm,
                      T *h_dists, int *h_medoid, double *h_means, double *h_sigmas, void *stream_v) {
   if (n < 1 || !h_series || !h_lens || !h_medoid || (n >= 2 && !h_dists))
@@ -224,6 +240,24 @@ int odba_tune_load(const char *path) {
 
 int odba_selftest_wait_timeout(uint64_t limit_ns, void *stream) {
   return gate_selftest(limit_ns, static_cast<cudaStream_t>(stream));
+}
+
+int odba_dtw_pairwise_range_f32(const float *series, const uint64_t *offsets, const uint64_t *lens,
+                                int n, uint64_t max_len, int use_open_start, int use_open_end,
+                                uint64_t pair_begin, uint64_t pair_end, float *dists,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  return pairwise_range_checked<float>(series, offsets, lens, n, max_len, use_open_start,
+                                       use_open_end, pair_begin, pair_end, dists, workspace,
+                                       workspace_bytes, stream);
+}
+
+int odba_dtw_pairwise_range_f64(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                                int n, uint64_t max_len, int use_open_start, int use_open_end,
+                                uint64_t pair_begin, uint64_t pair_end, double *dists,
+                                void *workspace, size_t workspace_bytes, void *stream) {
+  return pairwise_range_checked<double>(series, offsets, lens, n, max_len, use_open_start,
+                                        use_open_end, pair_begin, pair_end, dists, workspace,
+                                        workspace_bytes, stream);
 }
 
 int odba_dtw_pairwise_f32(const float *series, const uint64_t *offsets, const uint64_t *lens, int n,

@@ -37,7 +37,8 @@ struct PairwiseArgs {
   const uint64_t *offsets;
   const uint64_t *lens;
   int n;
-  unsigned long long npairs;
+  unsigned long long pbeg;    // first pair of the range (upper-triangle index)
+  unsigned long long npairs;  // pairs in the range
   T *dists;
   unsigned long long *counter;
   T *edges;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     if (lane == 0) q = atomicAdd(a.counter, 1ull);
     q = __shfl_sync(kFull, q, 0);
     if (q >= a.npairs) break;
-    const long long p = (long long)(a.npairs - 1 - q);
+    const long long p = (long long)(a.pbeg + a.npairs - 1 - q);
     int s, j;
     pair_of(p, a.n, s, j);
     SwathJob<T> job;
@@ -195,9 +196,10 @@ size_t whole_workspace_bytes(uint64_t max_len) {
 
 template <typename T, int RF>
 int whole_pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
-                          uint64_t max_len, int os, int oe, T *dists, void *workspace,
-                          size_t ws_bytes, cudaStream_t stream) {
-  if (n < 2) return ODBA_OK;
+                          uint64_t max_len, int os, int oe, unsigned long long pbeg,
+                          unsigned long long npairs, T *dists, void *workspace, size_t ws_bytes,
+                          cudaStream_t stream) {
+  if (n < 2 || npairs == 0) return ODBA_OK;
   const size_t need = whole_workspace_bytes<T>(max_len);
   if (ws_bytes < need) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "workspace too small");
   PairwiseArgs<T> a;
@@ -205,7 +207,8 @@ int whole_pairwise_launch(const T *series, const uint64_t *offsets, const uint64
   a.offsets = offsets;
   a.lens = lens;
   a.n = n;
-  a.npairs = (unsigned long long)n * (n - 1) / 2;
+  a.pbeg = pbeg;
+  a.npairs = npairs;
   a.dists = dists;
   a.counter = static_cast<unsigned long long *>(workspace);
   a.edges = reinterpret_cast<T *>(static_cast<char *>(workspace) + 256);
@@ -288,6 +291,7 @@ int pairwise_noalloc(const T *series, const uint64_t *offsets, const uint64_t *l
   a.offsets = offsets;
   a.lens = lens;
   a.n = n;
+  a.pbeg = 0;
   a.npairs = (unsigned long long)n * (n - 1) / 2;
   a.dists = dists;
   a.counter = static_cast<unsigned long long *>(scratch);
@@ -462,6 +466,7 @@ struct PipeArgs {
   const uint64_t *lens;
   int n;                         // series (all-vs-all) when list is null
   const odba_pair_task *list;    // pair list, or null for the upper triangle of n series
+  unsigned long long pbeg;       // first pair of the range (upper triangle only)
   unsigned long long npairs;
   unsigned long long max_swaths;
   T *dists;
@@ -505,7 +510,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
       oe = int((task.out >> 63) & 1ull);
       out = task.out & ((1ull << 62) - 1);
     } else {
-      const long long p = (long long)(a.npairs - 1 - qi);
+      const long long p = (long long)(a.pbeg + a.npairs - 1 - qi);
       pair_of(p, a.n, s, j);
       os = a.open_start;
       oe = a.open_end;
@@ -586,9 +591,9 @@ size_t swathpipe_workspace_bytes(unsigned long long npairs, uint64_t max_len) {
 
 template <typename T>
 int swathpipe_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
-                     const odba_pair_task *list, unsigned long long npairs, uint64_t max_len, int os,
-                     int oe, T *dists, void *workspace, size_t ws_bytes, cudaStream_t stream,
-                     unsigned long long limit_ns) {
+                     const odba_pair_task *list, unsigned long long pbeg, unsigned long long npairs,
+                     uint64_t max_len, int os, int oe, T *dists, void *workspace, size_t ws_bytes,
+                     cudaStream_t stream, unsigned long long limit_ns) {
   if (npairs == 0) return ODBA_OK;
   if (ws_bytes < swathpipe_workspace_bytes<T>(npairs, max_len))
     return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "workspace too small for the swath pipeline");
@@ -599,6 +604,7 @@ int swathpipe_launch(const T *series, const uint64_t *offsets, const uint64_t *l
   a.lens = lens;
   a.n = n;
   a.list = list;
+  a.pbeg = pbeg;
   a.npairs = npairs;
   a.max_swaths = (max_len + W - 1) / W;
   a.dists = dists;
@@ -621,11 +627,13 @@ int swathpipe_launch(const T *series, const uint64_t *offsets, const uint64_t *l
 template size_t swathpipe_workspace_bytes<float>(unsigned long long, uint64_t);
 template size_t swathpipe_workspace_bytes<double>(unsigned long long, uint64_t);
 template int swathpipe_launch<float>(const float *, const uint64_t *, const uint64_t *, int,
-                                     const odba_pair_task *, unsigned long long, uint64_t, int, int,
-                                     float *, void *, size_t, cudaStream_t, unsigned long long);
+                                     const odba_pair_task *, unsigned long long, unsigned long long,
+                                     uint64_t, int, int, float *, void *, size_t, cudaStream_t,
+                                     unsigned long long);
 template int swathpipe_launch<double>(const double *, const uint64_t *, const uint64_t *, int,
-                                      const odba_pair_task *, unsigned long long, uint64_t, int, int,
-                                      double *, void *, size_t, cudaStream_t, unsigned long long);
+                                      const odba_pair_task *, unsigned long long, unsigned long long,
+                                      uint64_t, int, int, double *, void *, size_t, cudaStream_t,
+                                      unsigned long long);
 
 }  // namespace odba
 
@@ -793,24 +801,37 @@ size_t pairwise_workspace_bytes_n(unsigned long long npairs, uint64_t max_len) {
 }
 
 template <typename T>
-int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
-                    uint64_t max_len, int os, int oe, T *dists, void *workspace, size_t ws_bytes,
-                    cudaStream_t stream) {
-  if (n < 2) return ODBA_OK;
-  const unsigned long long npairs = (unsigned long long)n * (n - 1) / 2;
+int pairwise_range_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                          uint64_t max_len, int os, int oe, unsigned long long pbeg,
+                          unsigned long long pend, T *dists, void *workspace, size_t ws_bytes,
+                          cudaStream_t stream) {
+  if (n < 2 || pend <= pbeg) return ODBA_OK;
+  const unsigned long long npairs = pend - pbeg;
   return run_planned<T>(npairs, max_len, ws_bytes, stream, [&](int plan) {
     switch (plan) {
       case ODBA_PLAN_WHOLE_PAIR_HALF_SWATH:
         return whole_pairwise_launch<T, Tune<T>::RF / 2>(series, offsets, lens, n, max_len, os, oe,
-                                                          dists, workspace, ws_bytes, stream);
+                                                          pbeg, npairs, dists, workspace, ws_bytes,
+                                                          stream);
       case ODBA_PLAN_SWATH_PIPELINE:
-        return swathpipe_launch<T>(series, offsets, lens, n, nullptr, npairs, max_len, os, oe,
+        return swathpipe_launch<T>(series, offsets, lens, n, nullptr, pbeg, npairs, max_len, os, oe,
                                    dists, workspace, ws_bytes, stream, 0);
       default:
         return whole_pairwise_launch<T, Tune<T>::RF>(series, offsets, lens, n, max_len, os, oe,
-                                                      dists, workspace, ws_bytes, stream);
+                                                      pbeg, npairs, dists, workspace, ws_bytes,
+                                                      stream);
     }
   });
+}
+
+template <typename T>
+int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                    uint64_t max_len, int os, int oe, T *dists, void *workspace, size_t ws_bytes,
+                    cudaStream_t stream) {
+  if (n < 2) return ODBA_OK;
+  return pairwise_range_launch<T>(series, offsets, lens, n, max_len, os, oe, 0,
+                                  (unsigned long long)n * (n - 1) / 2, dists, workspace, ws_bytes,
+                                  stream);
 }
 
 template <typename T>
@@ -824,7 +845,7 @@ int pairlist_launch(const T *series, const uint64_t *offsets, const uint64_t *le
         return whole_pairlist_launch<T, Tune<T>::RF / 2>(series, offsets, lens, tasks, ntasks,
                                                           max_len, dists, workspace, ws_bytes, stream);
       case ODBA_PLAN_SWATH_PIPELINE:
-        return swathpipe_launch<T>(series, offsets, lens, 0, tasks, ntasks, max_len, 0, 0, dists,
+        return swathpipe_launch<T>(series, offsets, lens, 0, tasks, 0, ntasks, max_len, 0, 0, dists,
                                    workspace, ws_bytes, stream, 0);
       default:
         return whole_pairlist_launch<T, Tune<T>::RF>(series, offsets, lens, tasks, ntasks, max_len,
@@ -957,6 +978,12 @@ template size_t pairwise_workspace_bytes_n<float>(unsigned long long, uint64_t);
 template size_t pairwise_workspace_bytes_n<double>(unsigned long long, uint64_t);
 template int pairwise_launch<float>(const float *, const uint64_t *, const uint64_t *, int,
                                     uint64_t, int, int, float *, void *, size_t, cudaStream_t);
+template int pairwise_range_launch<float>(const float *, const uint64_t *, const uint64_t *, int,
+                                          uint64_t, int, int, unsigned long long, unsigned long long,
+                                          float *, void *, size_t, cudaStream_t);
+template int pairwise_range_launch<double>(const double *, const uint64_t *, const uint64_t *, int,
+                                           uint64_t, int, int, unsigned long long, unsigned long long,
+                                           double *, void *, size_t, cudaStream_t);
 template int pairwise_launch<double>(const double *, const uint64_t *, const uint64_t *, int,
                                      uint64_t, int, int, double *, void *, size_t, cudaStream_t);
 template int pairlist_launch<float>(const float *, const uint64_t *, const uint64_t *,

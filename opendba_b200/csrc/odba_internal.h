@@ -27,6 +27,11 @@ int pairwise_launch(const T *series, const uint64_t *offsets, const uint64_t *le
                     cudaStream_t stream);
 
 template <typename T>
+int pairwise_range_launch(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
+                          uint64_t max_len, int os, int oe, unsigned long long pbeg,
+                          unsigned long long pend, T *dists, void *workspace, size_t ws_bytes,
+                          cudaStream_t stream);
+template <typename T>
 size_t pairwise_workspace_bytes_n(unsigned long long npairs, uint64_t max_len);
 
 // Autotuner of the pair kernels' launch plan (ODBA_PLAN_*).

@@ -63,3 +63,20 @@ def znorm_host(series: list[np.ndarray]) -> list[np.ndarray]:
         sd = x.std()
         out.append(((x - x.mean()) / (sd if sd != 0 else 1.0)).astype(s.dtype))
     return out
+
+
+def step_signals(rng: np.random.Generator, lens, level_mu: float, level_sd: float,
+                 dwell_mean: float, noise_sd: float, dtype=np.float32):
+    """Vectorised step_signal for many (long) series: geometric dwells with the
+    given mean, N(level_mu, level_sd) levels, N(0, noise_sd) noise."""
+    out = []
+    p = 1.0 / dwell_mean
+    for L in lens:
+        L = int(L)
+        dw = rng.geometric(p, size=int(L / dwell_mean * 1.1) + 16)
+        while dw.sum() < L:
+            dw = np.concatenate([dw, rng.geometric(p, size=int(L / dwell_mean * 0.2) + 16)])
+        levels = rng.normal(level_mu, level_sd, size=len(dw))
+        x = np.repeat(levels, dw)[:L] + rng.normal(0.0, noise_sd, size=L)
+        out.append(x.astype(dtype))
+    return out

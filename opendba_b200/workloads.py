@@ -168,3 +168,54 @@ def run_serving(rate_hz, n_requests=60, seed=0x0DBA0005, budget=32 << 30, detail
              "served_ms": 1e3 * l, "plain_ms": 1e3 * pd}
             for (k, d), rr, l, pd in zip(reqs, rounds, lats, plain_dur)]
     return out
+
+
+def run_long(n_series=16, len_lo=1_000_000, len_hi=4_000_000, dtypes=("f32", "f64"), minseg=4,
+             seed=0x0DBA0002 + 2):
+    """Few very long series: the k-segmentation DP on each raw series, then
+    all-vs-all DTW (global, z-normalised) in float32 and float64, which the
+    planner runs as the swath pipeline.  Device time by CUDA events."""
+    import torch
+    from . import _native
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(len_lo, len_hi + 1, size=n_series)
+    raw = synth.step_signals(rng, lens, 90.0, 12.0, 8.0, 1.5, np.float32)
+    raw.sort(key=len)
+    L = np.array([len(s) for s in raw], dtype=np.float64)
+    cells = float((L.sum() ** 2 - (L ** 2).sum()) / 2.0)
+    out = {"workload": f"{n_series} series, lengths U[{len_lo},{len_hi}], step signals (dwell 8, "
+                       f"noise 1.5), global DTW of all {n_series * (n_series - 1) // 2} pairs",
+           "samples": int(L.sum()), "cells": cells}
+    t0 = time.perf_counter()
+    segs = api.segment_host(raw, minseg)
+    out["segmentation"] = {"min_segment_length": minseg, "seconds": time.perf_counter() - t0,
+                           "segments": int(sum(len(s) for s in segs)),
+                           "msamples_per_s": L.sum() / (time.perf_counter() - t0) / 1e6,
+                           "api": "odba_segment_host_f32 (host series in, medians out)"}
+    lib = _native.lib()
+    for name in dtypes:
+        dt = np.float32 if name == "f32" else np.float64
+        ds = api.DeviceSeries.from_host([s.astype(dt) for s in raw])
+        api.znorm_(ds)
+        elem = np.dtype(dt).itemsize
+        ws = torch.empty(lib.odba_dtw_pairwise_workspace_bytes_n(elem, n_series, ds.max_len),
+                         dtype=torch.uint8, device="cuda")
+        import ctypes
+        plan = ctypes.c_int(0)
+        lib.odba_tune_query(elem, ds.max_len, n_series * (n_series - 1) // 2, ws.numel(),
+                            ctypes.addressof(plan), None)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        d = api.pairwise(ds, 0, 0, workspace=ws)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        err = int(ws[8:12].cpu().numpy().view(np.uint32)[0])
+        dh = d.cpu().numpy()
+        out[name] = {"seconds": ms / 1e3, "gcups": cells / ms / 1e6, "plan": plan.value,
+                     "workspace_gb": ws.numel() / 1e9, "wait_error": err,
+                     "finite": bool(np.isfinite(dh).all()), "checksum": float(dh.astype(np.float64).sum())}
+        del ds, ws, d
+        torch.cuda.empty_cache()
+    return out

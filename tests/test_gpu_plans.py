@@ -176,3 +176,42 @@ def test_bounded_wait_runs_out_and_reports(api):
     # the context is still usable afterwards
     ds = api.DeviceSeries.from_host([np.ones(40, np.float32), np.arange(50, dtype=np.float32)])
     assert np.isfinite(api.pairwise(ds).cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("plan", ["whole", "pipeline"])
+def test_pair_ranges_assemble_to_the_full_triangle(api, pin, plan):
+    import torch
+    from opendba_b200 import _native, sharding
+    rng = np.random.default_rng(17)
+    series = sorted([rng.standard_normal(int(L)).astype(np.float32)
+                     for L in rng.integers(500, 5000, size=30)], key=len)
+    ds = api.DeviceSeries.from_host(series)
+    n = len(series)
+    npairs = n * (n - 1) // 2
+    full = api.pairwise(ds, 0, 1).cpu().numpy()
+    ws = api.pairwise_workspace(ds)
+    out = torch.full((npairs,), float("nan"), dtype=torch.float32, device="cuda")
+    for b, e in sharding.shard_ranges([len(s) for s in series], 3):
+        pin(4, ds.max_len, max(e - b, 1), PLANS[plan])
+        _native.call("odba_dtw_pairwise_range_f32", ds.data.data_ptr(), ds.offsets.data_ptr(),
+                     ds.lens.data_ptr(), n, ds.max_len, 0, 1, b, e, out.data_ptr(), ws.data_ptr(),
+                     ws.numel(), None)
+    got = out.cpu().numpy()
+    assert np.array_equal(_bits(got), _bits(full))
+    from opendba_b200 import _native as N
+    with pytest.raises(N.OdbaError):
+        N.call("odba_dtw_pairwise_range_f32", ds.data.data_ptr(), ds.offsets.data_ptr(),
+               ds.lens.data_ptr(), n, ds.max_len, 0, 1, 5, npairs + 1, out.data_ptr(),
+               ws.data_ptr(), ws.numel(), None)
+
+
+def test_sharded_medoid_pass_single_rank(api):
+    from opendba_b200 import sharding
+    rng = np.random.default_rng(21)
+    series = sorted([rng.standard_normal(int(L)).astype(np.float32)
+                     for L in rng.integers(300, 2000, size=25)], key=len)
+    ds = api.DeviceSeries.from_host(series)
+    full, med = sharding.medoid_pass_sharded(ds, [len(s) for s in series], 0, 1)
+    want = O.pairwise(series, 0, 0, fma_mode=1)
+    assert np.array_equal(_bits(full.cpu().numpy()), _bits(want))
+    assert med == O.medoid(want, np.array([len(s) for s in series], dtype=np.uint64))[0]
