@@ -166,6 +166,30 @@ int odba_dtw_pairwise_noalloc_f32(const float *series, const uint64_t *offsets,
                                   int use_open_start, int use_open_end, float *dists,
                                   void *stream);
 
+/* ---- clustering of the medoid pass --------------------------------------------
+ * Replaces the clustering half of approximateMedoidIndices (dba.hpp:219-343)
+ * and the hclust-cpp calls it makes (hclust_fast with complete linkage,
+ * cutree_k, cutree_cdist; dba.hpp:234, 248, 276).  Host memory throughout.
+ * odba_complete_linkage: dists is the condensed upper triangle (n(n-1)/2
+ * doubles, reference pair order); merge (2(n-1) ints, column-major (n-1) x 2)
+ * and height (n-1) follow R's hclust convention (singleton x as -(x+1),
+ * cluster of step k as k+1, heights ascending).  odba_cutree_k labels the n
+ * leaves after the first n-k merges, clusters numbered by their lowest leaf
+ * (k < 2 or k > n: one cluster); odba_cutree_cdist applies the merges below
+ * height cdist.  odba_cluster_medoids_*: from the T distance triangle and the
+ * lengths, the memberships and per-cluster medoids for a clustering threshold
+ * cdist with the reference's meaning (1: one cluster; > 1: that many
+ * clusters, raised until enough have several members; [0, 1): cut height on
+ * distances scaled by the largest; negative: one cluster, the reference
+ * leaves it unimplemented); medoids needs n ints. */
+int odba_complete_linkage(int n, const double *dists, int *merge, double *height);
+int odba_cutree_k(int n, const int *merge, int k, int *labels);
+int odba_cutree_cdist(int n, const int *merge, const double *height, double cdist, int *labels);
+int odba_cluster_medoids_f32(int n, const float *dists, const uint64_t *lens, double cdist,
+                             int *memberships, int *medoids, int *num_clusters);
+int odba_cluster_medoids_f64(int n, const double *dists, const uint64_t *lens, double cdist,
+                             int *memberships, int *medoids, int *num_clusters);
+
 /* ---- medoid from pair distances (one cluster) ------------------------------
  * Replaces the sum-of-squares and medoid choice of approximateMedoidIndices
  * (dba.hpp:186-203, 325-342).  sos (n values) and medoid (one int) are device

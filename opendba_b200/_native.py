@@ -34,6 +34,11 @@ SIGNATURES = {
     "odba_dtw_pairwise_workspace_bytes_n": (ctypes.c_size_t, [I32, I32, U64]),
     "odba_dtw_pairwise_range_f32": (I32, [P, P, P, I32, U64, I32, I32, U64, U64, P, P, ctypes.c_size_t, P]),
     "odba_dtw_pairwise_range_f64": (I32, [P, P, P, I32, U64, I32, I32, U64, U64, P, P, ctypes.c_size_t, P]),
+    "odba_complete_linkage": (I32, [I32, P, P, P]),
+    "odba_cutree_k": (I32, [I32, P, I32, P]),
+    "odba_cutree_cdist": (I32, [I32, P, P, ctypes.c_double, P]),
+    "odba_cluster_medoids_f32": (I32, [I32, P, P, ctypes.c_double, P, P, P]),
+    "odba_cluster_medoids_f64": (I32, [I32, P, P, ctypes.c_double, P, P, P]),
     "odba_tune_set": (I32, [I32, I32, I32, I32]),
     "odba_tune_query": (I32, [I32, U64, U64, ctypes.c_size_t, P, P]),
     "odba_tune_mode": (None, [I32]),

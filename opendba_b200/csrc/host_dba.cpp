@@ -377,34 +377,25 @@ int *medoid_pass(const T *d_data, const uint64_t *d_offs, const uint64_t *d_lens
   for (int pad = 0; pad < n; ++pad) mats << "\t";
   mats << "0" << std::endl;
   mats.close();
-  if (*cdist != 1) {
-    std::cerr << "Clustering thresholds other than 1 (complete linkage) are not available in this "
-                 "build; use 1 for a single consensus"
-              << std::endl;
-    die(odba_exit::MEDOID_FINDING_ERROR);
+  // complete linkage, the cut and the per-cluster medoids (dba.hpp:219-343)
+  std::vector<int> med(std::max(n, 1), -1);
+  int num_clusters = 1;
+  check(sizeof(T) == 4
+            ? odba_cluster_medoids_f32(n, reinterpret_cast<const float *>(dists.data()), h_lens.data(),
+                                       *cdist, memberships, med.data(), &num_clusters)
+            : odba_cluster_medoids_f64(n, reinterpret_cast<const double *>(dists.data()), h_lens.data(),
+                                       *cdist, memberships, med.data(), &num_clusters),
+        "clustering");
+  std::cerr << "There are " << num_clusters << " clusters" << std::endl;
+  int *medoids = new int[num_clusters];
+  for (int c = 0; c < num_clusters; ++c) {
+    if (med[c] == -1) {
+      std::cerr << "Logic error in medoid finding routine" << std::endl;
+      die(odba_exit::MEDOID_FINDING_ERROR);
+    }
+    medoids[c] = med[c];
+    std::cerr << "Processing cluster " << c << " medoid is " << med[c] << std::endl;
   }
-  for (int i = 0; i < n; ++i) memberships[i] = 0;
-  std::cerr << "There are 1 clusters" << std::endl;
-  int *medoids = new int[1];
-  int medoid = -1;
-  if (n > 2) {
-    T lowest = std::numeric_limits<T>::max();
-    for (int i = 0; i < n; ++i)
-      if (sos[i] < lowest) {
-        medoid = i;
-        lowest = sos[i];
-      }
-  } else if (n == 2) {
-    medoid = h_lens[0] > h_lens[1] ? 0 : 1;
-  } else {
-    medoid = 0;
-  }
-  if (medoid == -1) {
-    std::cerr << "Logic error in medoid finding routine" << std::endl;
-    die(odba_exit::MEDOID_FINDING_ERROR);
-  }
-  std::cerr << "Processing cluster 0 membership=" << n << ", medoid is " << medoid << std::endl;
-  medoids[0] = medoid;
   return medoids;
 }
 

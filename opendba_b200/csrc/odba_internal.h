@@ -50,6 +50,14 @@ int pairlist_launch(const T *series, const uint64_t *offsets, const uint64_t *le
                     const odba_pair_task *tasks, unsigned long long ntasks, uint64_t max_len,
                     T *dists, void *workspace, size_t ws_bytes, cudaStream_t stream);
 
+// Complete linkage and dendrogram cuts (clustering.cpp, host code).
+void complete_linkage(int n, double *D, int *merge, double *height);
+void cut_tree_k(int n, const int *merge, int k, int *labels);
+void cut_tree_height(int n, const int *merge, const double *height, double cdist, int *labels);
+template <typename T>
+int cluster_and_medoids(int n, const T *dists, const uint64_t *lens, double cdist, int *memberships,
+                        int *medoids);
+
 template <typename T>
 int medoid_launch(const T *dists, const uint64_t *lens, int n, T *sos, int *medoid,
                   cudaStream_t stream);

@@ -23,8 +23,8 @@
 //   znorm      <in.odbs> <out_prefix>
 //       normalizeSequences (gpu_utils.hpp:132-170): writes the normalised
 //       series, and the per-series means and sigmas (float64).
-//   performdba <in.odbs> <out_prefix> <open_start> <open_end> <norm>
-//       performDBA (dba.hpp:863-1189), CLUSTER_AND_CONSENSUS, cdist = 1.
+//   performdba <in.odbs> <out_prefix> <open_start> <open_end> <norm> [cdist]
+//       performDBA (dba.hpp:863-1189), CLUSTER_AND_CONSENSUS, cdist default 1.
 //   setupandrun <out_prefix> <open_start> <open_end> <norm> <file>...
 //       setupAndRun<float> on text files, as tests/openDBA_test.cu does.
 //   segment    <in.odbs> <out.odbs> <min_segment_length> <prefix_skip>
@@ -217,14 +217,15 @@ static int run_znorm(const SeriesBundle &b, const std::string &prefix) {
 }
 
 template <typename T>
-static int run_performdba(const SeriesBundle &b, const std::string &prefix, int os, int oe, int norm) {
+static int run_performdba(const SeriesBundle &b, const std::string &prefix, int os, int oe, int norm,
+                          double cdist) {
   size_t *lens = nullptr;
   T **seqs = managed_series<T>(b, &lens);
   char **names = make_names(b.n());
   std::vector<char> pfx(prefix.begin(), prefix.end());
   pfx.push_back('\0');
   char *files[1] = {pfx.data()};
-  performDBA<T>(seqs, (int)b.n(), lens, names, os, oe, pfx.data(), norm, 1.0, files, 1,
+  performDBA<T>(seqs, (int)b.n(), lens, names, os, oe, pfx.data(), norm, cdist, files, 1,
                 BINARY_READ_MODE, false, CLUSTER_AND_CONSENSUS);
   cudaDeviceSynchronize();
   CUERR("harness: performDBA sync");
@@ -289,9 +290,10 @@ int main(int argc, char **argv) {
     } else if (mode == "znorm") {
       rc = dbl ? run_znorm<double>(b, argv[3]) : run_znorm<float>(b, argv[3]);
     } else if (mode == "performdba") {
-      if (argc < 7) die("performdba <in> <prefix> <os> <oe> <norm>");
-      rc = dbl ? run_performdba<double>(b, argv[3], std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]))
-               : run_performdba<float>(b, argv[3], std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]));
+      if (argc < 7) die("performdba <in> <prefix> <os> <oe> <norm> [cdist]");
+      const double cdist = argc > 7 ? std::atof(argv[7]) : 1.0;
+      rc = dbl ? run_performdba<double>(b, argv[3], std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]), cdist)
+               : run_performdba<float>(b, argv[3], std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]), cdist);
     } else if (mode == "segment") {
       if (argc < 6) die("segment <in> <out> <minseg> <skip>");
       rc = dbl ? run_segment<double>(b, argv[3], std::atoi(argv[4]), std::atoi(argv[5]))

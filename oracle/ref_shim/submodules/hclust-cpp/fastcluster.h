@@ -5,9 +5,8 @@
 // declares the three entry points at the reference's call sites
 // (dba.hpp:234 hclust_fast, dba.hpp:248 cutree_k, dba.hpp:276 cutree_cdist)
 // so that the reference harness in oracle/ref_harness.cu links.  The matching
-// definitions in oracle/ref_hclust_stub.cpp are placeholders that are only
-// valid for a clustering threshold of exactly 1, where the reference ignores
-// the dendrogram (dba.hpp:266-272).
+// definitions in oracle/ref_hclust_shim.cpp forward to this project's
+// complete linkage (opendba_b200/csrc/clustering.cpp).
 #ifndef ODBA_REF_SHIM_FASTCLUSTER_H
 #define ODBA_REF_SHIM_FASTCLUSTER_H
 

@@ -7,7 +7,7 @@ committed copy lives in tests/golden/ref/; tests compare the CUDA path and
 the CPU oracle against it.
 
 Run on a B200 box from the repository root:
-    python tests/golden/make_reference_golden.py [out_dir]
+    python tests/golden/make_reference_golden.py [out_dir] [--clusters-only]
 """
 from __future__ import annotations
 
@@ -81,11 +81,50 @@ def gz(src, dst):
         g.write(f.read())
 
 
+def family_series(dtype, seed, n_per=(9, 8, 7)):
+    """Three families of warped, noisy copies of three random-walk templates."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for f, cnt in enumerate(n_per):
+        tmpl = np.cumsum(rng.standard_normal(600)) + 80.0 + 15.0 * f
+        for _ in range(cnt):
+            L = int(rng.integers(300, 900))
+            t = np.sort(rng.random(L)) * (len(tmpl) - 1)
+            x = np.interp(t, np.arange(len(tmpl)), tmpl) + rng.normal(0, 0.8, L)
+            out.append(x.astype(dtype))
+    order = rng.permutation(len(out))
+    return [out[i] for i in order]
+
+
+def cluster_cases(out, tmp, log):
+    """performDBA with clustering thresholds other than 1 (dba.hpp:219-343,
+    951-962): membership file, per-cluster averages and pair distances."""
+    cases = [(np.float32, "f32", "global", 0.3), (np.float32, "f32", "global", 3.0),
+             (np.float32, "f32", "global", 0.0), (np.float64, "f64", "open_end", 0.45)]
+    for dt, sfx, mode, cdist in cases:
+        ser = family_series(dt, synth.SEED_BASE + 505)
+        name = f"cluster_{sfx}_{mode}_c{cdist:g}"
+        O.write_bundle(os.path.join(out, f"cluster_{sfx}.odbs"), ser)
+        pfx = os.path.join(tmp, name)
+        os_, oe = MODES[mode]
+        run(["performdba", os.path.join(out, f"cluster_{sfx}.odbs"), pfx, os_, oe, 1, cdist], log)
+        for ext in (".avg.txt", ".pair_dists.txt", ".cluster_membership.txt"):
+            if os.path.exists(pfx + ext):
+                shutil.copy(pfx + ext, os.path.join(out, name + ext))
+
+
 def main():
-    out = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden_ref"))
+    out = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--")
+                          else os.path.join(ROOT, "gpurun_out", "golden_ref"))
     os.makedirs(out, exist_ok=True)
     tmp = os.path.join(out, "_tmp")
     os.makedirs(tmp, exist_ok=True)
+    if "--clusters-only" in sys.argv:
+        with open(os.path.join(out, "harness_log_clusters.jsonl"), "w") as log:
+            cluster_cases(out, tmp, log)
+        shutil.rmtree(tmp, ignore_errors=True)
+        print("cluster golden written to", out)
+        return
     log = open(os.path.join(out, "harness_log.jsonl"), "w")
     meta = {"harness": "oracle/_ref/ref_harness", "modes": MODES}
 
@@ -183,11 +222,15 @@ def main():
             run(["segment", os.path.join(out, f"seg_{sfx}.odbs"),
                  os.path.join(out, f"seg_{sfx}_m{minseg}.odbs"), minseg, 0], log)
 
+    # 8. clustering thresholds other than 1
+    with open(os.path.join(out, "harness_log_clusters.jsonl"), "w") as clog:
+        cluster_cases(out, tmp, clog)
+
     with open(os.path.join(out, "meta.json"), "w") as f:
         json.dump(meta, f, indent=1)
     shutil.rmtree(tmp, ignore_errors=True)
 
-    # 8. timing only (not a fixture): the reference's medoid launches on the first
+    # 9. timing only (not a fixture): the reference's medoid launches on the first
     # 40 rows of the 2000-series nanopore-like workload.
     if "--timing" in sys.argv:
         c2 = synth.znorm_host(synth.nanopore_like(2000, 2000, 8000, synth.SEED_BASE + 2))

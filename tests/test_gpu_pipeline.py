@@ -162,3 +162,23 @@ def test_cli_rejects_bad_arguments(built, tmp_path):
     p = subprocess.run([cli, "text", "float", "global", str(tmp_path / "x"), "0", "/dev/null", "1",
                         str(tmp_path / "missing.txt")], capture_output=True, text=True)
     assert p.returncode == 32  # NOT_ENOUGH_SEQUENCES
+
+
+@pytest.mark.parametrize("tag", ["f32_global_c0.3", "f32_global_c3", "f32_global_c0", "f64_open_end_c0.45"])
+def test_perform_dba_clusters_byte_identical(built, tmp_path, tag):
+    # clustering thresholds other than 1: the reference's run (with this
+    # project's complete linkage in place of hclust-cpp) gives the golden files
+    sfx, rest = tag.split("_", 1)
+    mode, c = rest.rsplit("_c", 1)
+    gold = os.path.join(GOLDEN, f"cluster_{tag}")
+    if not os.path.exists(gold + ".avg.txt"):
+        pytest.skip("cluster golden files not generated")
+    src = os.path.join(GOLDEN, f"cluster_{sfx}.odbs")
+    prefix = str(tmp_path / f"cluster_{tag}")
+    os_, oe = {"global": (0, 0), "open_end": (0, 1)}[mode]
+    _child("from oracle import oracle as O\nfrom opendba_b200 import api\n"
+           f"s = O.read_bundle({src!r})\n"
+           f"api.perform_dba(s, ['s%d' % i for i in range(len(s))], {prefix!r}, {os_}, {oe}, norm=1, "
+           f"cdist={float(c)})")
+    for ext in (".cluster_membership.txt", ".avg.txt", ".pair_dists.txt"):
+        assert _read(prefix + ext) == _read(gold + ext), ext
