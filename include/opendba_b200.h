@@ -234,6 +234,37 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
                        int64_t *path_counts, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* ---- one DBA round in stripe mode ------------------------------------------------
+ * Replaces DBAUpdate<T>'s stripe mode (dba.hpp:515-763), used by the
+ * reference when a member's path matrix does not fit in device memory.  Same
+ * arguments and results as odba_dba_round_* (bit for bit), but no member's
+ * path is ever held whole: the forward pass keeps every swath's right edge
+ * and every ckpt_rows-th cost row (a power of two; 0 = 4096), and the
+ * backtrack recomputes, swath by swath from the right, the tiles of
+ * ckpt_rows rows below the path in parallel.  Workspace for the longest
+ * member m and centroid length Lc: about (Lc/1024 * m + m/ckpt_rows * Lc)
+ * values plus m * 256 bytes (float; double swaths are 512 wide) -- 80 GB
+ * for 4 M x 4 M in float with the default, where a full path needs 4 TB.
+ * Global and open-start alignment only (ODBA_ERR_INVALID_ARGUMENT with an
+ * open end): there the reference's stripe mode gives its full-path results;
+ * with an open end its stripe recompute applies the open-end rules at the
+ * backtrack height instead of the last row, which is not reproduced. */
+size_t odba_dba_round_stripe_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
+                                             uint64_t centroid_len, int use_open_start,
+                                             int ckpt_rows);
+int odba_dba_round_stripe_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int ckpt_rows,
+                              float *new_centroid, uint32_t *counts, double *delta,
+                              int32_t *path_triples, int64_t *path_counts, void *workspace,
+                              size_t workspace_bytes, void *stream);
+int odba_dba_round_stripe_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int ckpt_rows,
+                              double *new_centroid, uint32_t *counts, double *delta,
+                              int32_t *path_triples, int64_t *path_counts, void *workspace,
+                              size_t workspace_bytes, void *stream);
+
 /* ---- one DBA round for many jobs at once ---------------------------------------
  * No single reference counterpart: DBAUpdate<T> (dba.hpp:432-848) for many
  * independent averaging jobs in one launch sequence (no host synchronization
@@ -247,9 +278,12 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
  * (optional) is the order in which members are aligned (longest first keeps
  * the tail short); it does not change any result.  Outputs per job at the
  * job's centroid offset: means, counts; deltas[J] = max |centroid - mean|.
- * The h_* arrays are host copies that size the workspace.  Results equal one
- * odba_dba_round_* call per job, bit for bit.  series may be NULL, with
- * offsets as element addresses (see odba_dtw_pairlist_*). */
+ * The h_* arrays are host copies that size the workspace: only jobs whose
+ * h_job_flags have bit 2 set take path and range space, so a large set of
+ * jobs can run in waves with a workspace sized for one wave (the device flags
+ * of a launch must then activate no job outside the sizing set).  Results
+ * equal one odba_dba_round_* call per job, bit for bit.  series may be NULL,
+ * with offsets as element addresses (see odba_dtw_pairlist_*). */
 size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_lens,
                                       const int *h_member_job, int nmem,
                                       const uint64_t *h_centroid_lens, const int *h_job_flags,

@@ -145,12 +145,14 @@ def medoid_pass_host(series, open_start: int = 0, open_end: int = 0, norm: int =
 
 
 def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: int = 0,
-              with_paths: bool = False, workspace=None, stream=None):
+              with_paths: bool = False, workspace=None, stream=None, stripe_rows=None):
     """One DBA round of ``members`` against ``centroid`` (DBAUpdate, dba.hpp:434).
 
     centroid: device tensor (same dtype as members).  Returns (new_centroid,
     counts, delta, paths) where paths is None or a list of (k, 3) int32 numpy
-    arrays (row, column, move) in the order of the reference's path files."""
+    arrays (row, column, move) in the order of the reference's path files.
+    stripe_rows: None for the full-path round, else the stripe-mode round with
+    that many rows per recomputed tile (a power of two; 0 = the default)."""
     torch = _torch()
     Lc = int(centroid.numel())
     dev = members.data.device
@@ -158,8 +160,13 @@ def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: in
     h_lens = np.ascontiguousarray(members.host_lens, dtype=np.uint64)
     vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     if workspace is None:
-        nbytes = lib.odba_dba_round_workspace_bytes(members.dtype.itemsize, vp(h_lens), members.n,
-                                                    Lc, int(open_start), int(open_end))
+        if stripe_rows is None:
+            nbytes = lib.odba_dba_round_workspace_bytes(members.dtype.itemsize, vp(h_lens),
+                                                        members.n, Lc, int(open_start), int(open_end))
+        else:
+            nbytes = lib.odba_dba_round_stripe_workspace_bytes(members.dtype.itemsize, vp(h_lens),
+                                                               members.n, Lc, int(open_start),
+                                                               int(stripe_rows))
         workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     mean = torch.empty(Lc, dtype=members.data.dtype, device=dev)
     counts = torch.empty(Lc, dtype=torch.int32, device=dev)
@@ -169,9 +176,14 @@ def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: in
         cap = int(h_lens.sum()) + members.n * (Lc + 1)
         tri = torch.empty(3 * cap, dtype=torch.int32, device=dev)
         cnt = torch.empty(members.n, dtype=torch.int64, device=dev)
-    _native.call(f"odba_dba_round_{_SFX[members.dtype]}", centroid.data_ptr(), Lc,
+    mode_args = (int(open_start), int(open_end))
+    name = f"odba_dba_round_{_SFX[members.dtype]}"
+    if stripe_rows is not None:
+        mode_args += (int(stripe_rows),)
+        name = f"odba_dba_round_stripe_{_SFX[members.dtype]}"
+    _native.call(name, centroid.data_ptr(), Lc,
                  members.data.data_ptr(), members.offsets.data_ptr(), members.lens.data_ptr(),
-                 vp(h_lens), members.n, int(open_start), int(open_end), mean.data_ptr(),
+                 vp(h_lens), members.n, *mode_args, mean.data_ptr(),
                  counts.data_ptr(), delta.data_ptr(), tri.data_ptr() if tri is not None else None,
                  cnt.data_ptr() if cnt is not None else None, workspace.data_ptr(),
                  workspace.numel(), _stream_ptr(stream))

@@ -161,7 +161,8 @@ int dba_round_checked(const T *centroid, uint64_t Lc, const T *series,
                              const uint64_t *offsets, const uint64_t *lens,
                              const uint64_t *h_lens, int n, int os, int oe, T *mean,
                              uint32_t *counts, double *delta, int32_t *triples,
-                             int64_t *triple_counts, void *ws, size_t ws_bytes, void *stream) {
+                             int64_t *triple_counts, void *ws, size_t ws_bytes, void *stream,
+                             int ckpt_rows = -1) {
   if (n < 1 || Lc == 0 || !centroid || !series || !offsets || !lens || !h_lens || !mean ||
       !counts || !delta || !ws)
     return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer, empty centroid or no members");
@@ -172,6 +173,10 @@ int dba_round_checked(const T *centroid, uint64_t Lc, const T *series,
       return fail(ODBA_ERR_INVALID_ARGUMENT, "member lengths must be in [1, 2^30]");
   if (Lc > (1ull << 30)) return fail(ODBA_ERR_INVALID_ARGUMENT, "centroid too long");
   if (int rc = require_sm100()) return rc;
+  if (ckpt_rows >= 0)
+    return dba_round_stripe_launch<T>(centroid, Lc, series, offsets, lens, h_lens, n, os ? 1 : 0,
+                                      oe ? 1 : 0, ckpt_rows, mean, counts, delta, triples,
+                                      triple_counts, ws, ws_bytes, static_cast<cudaStream_t>(stream));
   return dba_round_launch<T>(centroid, Lc, series, offsets, lens, h_lens, n, os ? 1 : 0,
                              oe ? 1 : 0, mean, counts, delta, triples, triple_counts, ws,
                              ws_bytes, static_cast<cudaStream_t>(stream));
@@ -369,6 +374,41 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
   return dba_round_checked<double>(centroid, centroid_len, series, offsets, lens, h_lens, n,
                                    use_open_start, use_open_end, new_centroid, counts, delta,
                                    path_triples, path_counts, workspace, workspace_bytes, stream);
+}
+
+size_t odba_dba_round_stripe_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
+                                             uint64_t centroid_len, int use_open_start,
+                                             int ckpt_rows) {
+  if (n < 1 || !h_lens || centroid_len == 0) return 0;
+  if (elem_size == 8)
+    return dba_round_stripe_workspace_bytes<double>(h_lens, n, centroid_len, use_open_start, ckpt_rows);
+  return dba_round_stripe_workspace_bytes<float>(h_lens, n, centroid_len, use_open_start, ckpt_rows);
+}
+
+int odba_dba_round_stripe_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int ckpt_rows,
+                              float *new_centroid, uint32_t *counts, double *delta,
+                              int32_t *path_triples, int64_t *path_counts, void *workspace,
+                              size_t workspace_bytes, void *stream) {
+  if (ckpt_rows < 0) return fail(ODBA_ERR_INVALID_ARGUMENT, "checkpoint rows must be >= 0");
+  return dba_round_checked<float>(centroid, centroid_len, series, offsets, lens, h_lens, n,
+                                  use_open_start, use_open_end, new_centroid, counts, delta,
+                                  path_triples, path_counts, workspace, workspace_bytes, stream,
+                                  ckpt_rows);
+}
+
+int odba_dba_round_stripe_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int ckpt_rows,
+                              double *new_centroid, uint32_t *counts, double *delta,
+                              int32_t *path_triples, int64_t *path_counts, void *workspace,
+                              size_t workspace_bytes, void *stream) {
+  if (ckpt_rows < 0) return fail(ODBA_ERR_INVALID_ARGUMENT, "checkpoint rows must be >= 0");
+  return dba_round_checked<double>(centroid, centroid_len, series, offsets, lens, h_lens, n,
+                                   use_open_start, use_open_end, new_centroid, counts, delta,
+                                   path_triples, path_counts, workspace, workspace_bytes, stream,
+                                   ckpt_rows);
 }
 
 size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_lens,

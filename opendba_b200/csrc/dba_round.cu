@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "dtw_path.cuh"
+#include "dtw_pipe.cuh"
 #include "odba_internal.h"
 
 namespace odba {
@@ -108,6 +109,10 @@ __device__ __forceinline__ MemberGeom geom_of(const RoundArgs<T> &a, int k, int 
   return member_geom<T>(a.lens[a.mseries[k]], uint64_t(a.clen[job]), f & 1, (f >> 1) & 1);
 }
 
+// Members of inactive jobs take no path words and no ranges (a caller can run
+// a large set of jobs in waves with a workspace sized for one wave); the path
+// listing keeps a slot for every member so its layout does not depend on the
+// flags.
 template <typename T>
 __global__ void plan_kernel(RoundArgs<T> a) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -118,8 +123,9 @@ __global__ void plan_kernel(RoundArgs<T> a) {
     a.path_off[k] = w;
     a.trip_off[k] = p;
     a.rng_off[k] = r;
-    w += g.words;
     p += (unsigned long long)(g.m + g.n + 1);
+    if (!(a.jflags[job] & 4)) continue;
+    w += g.words;
     r += (unsigned long long)a.clen[job];
   }
   for (int j = 0; j < a.njobs; ++j)
@@ -455,6 +461,7 @@ void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint
   for (int k = 0; k < nmem; ++k) {
     const int j = h_mjob ? h_mjob[k] : 0;
     const int f = h_flags[j];
+    if (!(f & 4)) continue;
     const MemberGeom g = member_geom<T>(h_lens[k], h_clen[j], f & 1, (f >> 1) & 1);
     words += g.words;
     ranges += h_clen[j];
@@ -588,6 +595,489 @@ int dba_batch_launch(const T *centroids, const unsigned long long *coff, const i
   a.triple_counts = triple_counts;
   return launch_round<T>(a, L, static_cast<char *>(ws), max_clen, stream);
 }
+
+// ---------------------------------------------------------------------------
+// Stripe mode: one DBA round for members whose 2-bit path does not fit in
+// memory (the reference's stripe mode, dba.hpp:515-763).  Per member:
+//   1. forward: the swath pipeline (many warps, bounded hand-off waits) over
+//      the member's swaths; every swath's right edge is kept (E, one column of
+//      rows per swath) and every K-th cost row is kept across all columns (Q);
+//   2. backtrack, swath by swath from the right: every K-row tile of the swath
+//      below the current backtrack height is recomputed with its moves in
+//      parallel (one warp per tile: its row below comes from Q, its left edge
+//      from E), then one thread continues the walk through the swath and
+//      records the per-centroid-index sample ranges (and the path listing)
+//      exactly as the full-path backtrack does;
+//   3. the ordered reducer of the full-path round.
+// Recomputed costs equal the forward costs cell for cell, so paths, sums and
+// the delta are bit-identical to the full-path round.  Global and open-start
+// alignment only: there the reference's stripe mode gives its full-path
+// results too; with an open end its stripe recompute applies the open-end
+// rules at the backtrack height instead of the last row (dtw.hpp:74-129 with
+// first_seq_length set to the backtrack height), which is not reproduced.
+namespace {
+
+struct StripeWalk {
+  int r, c, h, cur_t, lo, hi, state;  // state: 0 walking, 1 done, 2 failed
+  long long nt;
+};
+
+template <typename T>
+struct StripeArgs {
+  const T *series;
+  const uint64_t *offsets;
+  int member;                   // x = series + offsets[member]
+  const T *y;                   // centroid (columns)
+  int m, n, r0, swaths, shift;  // tile height K = 1 << shift
+  T *E;
+  unsigned long long e_stride;
+  T *Q;
+  unsigned long long q_stride;
+  unsigned long long *prog;     // one progress word per swath
+  unsigned *err;
+  unsigned long long *counter;
+  unsigned long long *words;    // one swath of moves, full-path layout
+  StripeWalk *walk;
+  int2 *ranges;                 // this member's ranges (n of them)
+  int32_t *triples;             // this member's path listing, or null
+  int64_t *triple_count;        // or null
+  unsigned long long limit_ns;
+};
+
+// Registers per lane of swath s (the last, partial swath is narrower).
+template <typename T>
+__host__ __device__ inline int stripe_regs(int n, int s) {
+  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
+  const int c0 = s * W;
+  const int width = n - c0 < W ? n - c0 : W;
+  const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
+  return rq < RF ? rq : RF;
+}
+
+template <typename T>
+__device__ __forceinline__ T stripe_corner(int c0, int r0) {
+  return c0 == 0 ? (r0 ? Num<T>::big() : T(0)) : (r0 ? T(0) : Num<T>::big());
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void stripe_fwd_swath(const SwathJob<T> &job, const PipeGate &gate,
+                                                 const CkptOut<T> &ck) {
+  T col[R];
+  sweep_swath<T, R, PipeGate, true>(job, col, gate, ck);
+}
+
+template <typename T, int RF, int RQ>
+__global__ void __launch_bounds__(kRoundWarps * 32) stripe_forward_kernel(StripeArgs<T> a) {
+  __shared__ __align__(16) T stage_mem[kRoundWarps * kStageElems];
+  constexpr int W = 32 * RF;
+  const int lane = threadIdx.x & 31;
+  const T *x = a.series + a.offsets[a.member];
+  for (;;) {
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(a.counter, 1ull);
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= (unsigned long long)a.swaths) break;
+    const int sw = int(q), c0 = sw * W;
+    SwathJob<T> job;
+    job.x = x;
+    job.y = a.y;
+    job.m = a.m;
+    job.n = a.n;
+    job.c0 = c0;
+    job.r0 = a.r0;
+    job.edge_in = sw ? a.E + (unsigned long long)(sw - 1) * a.e_stride : nullptr;
+    job.edge_out = sw + 1 < a.swaths ? a.E + (unsigned long long)sw * a.e_stride : nullptr;
+    job.open_end = false;
+    job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
+    job.corner_init = stripe_corner<T>(c0, a.r0);
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
+    PipeGate gate;
+    gate.prog_in = a.prog + (sw ? sw - 1 : 0);
+    gate.prog_out = a.prog + sw;
+    gate.err = a.err;
+    gate.limit_ns = a.limit_ns;
+    gate.avail = 0;
+    const CkptOut<T> ck{a.Q + c0, a.q_stride, a.shift};
+    const int R = stripe_regs<T>(a.n, sw);
+    if (R == RF) {
+      stripe_fwd_swath<T, RF>(job, gate, ck);
+    } else {
+      switch (R / RQ) {
+#define ODBA_SCASE(K)                                                         \
+  case K:                                                                     \
+    if constexpr (K * RQ < RF) stripe_fwd_swath<T, K * RQ>(job, gate, ck);    \
+    break;
+        ODBA_SCASE(1)
+        ODBA_SCASE(2)
+        ODBA_SCASE(3)
+        ODBA_SCASE(4)
+        ODBA_SCASE(5)
+        ODBA_SCASE(6)
+        ODBA_SCASE(7)
+#undef ODBA_SCASE
+        default:
+          break;
+      }
+    }
+  }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void stripe_tile_swath(const SwathJob<T> &job, const PathOut &po,
+                                                  const TileIn<T> &tile) {
+  T col[R];
+  T emin, etop;
+  sweep_swath_path<T, R>(job, po, col, emin, etop, tile);
+}
+
+// One warp per K-row tile of swath s below the backtrack height.
+template <typename T, int RF, int RQ>
+__global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArgs<T> a, int s) {
+  constexpr int W = 32 * RF;
+  const int kt = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
+  const int H = a.walk->h;
+  const int K = 1 << a.shift;
+  const long long rb_l = (long long)a.r0 + (long long)kt * K;
+  if (a.walk->state != 0 || rb_l >= H) return;
+  const int rb = int(rb_l);
+  const int re = rb + K < H ? rb + K : H;
+  const int c0 = s * W;
+  SwathJob<T> job;
+  job.x = a.series + a.offsets[a.member];
+  job.y = a.y;
+  job.m = re;
+  job.n = a.n;
+  job.c0 = c0;
+  job.r0 = rb;
+  const T *left = s ? a.E + (unsigned long long)(s - 1) * a.e_stride : nullptr;
+  job.edge_in = left ? left + (unsigned long long)kt * K : nullptr;
+  job.edge_out = nullptr;
+  job.open_end = false;
+  job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
+  job.corner_init = kt == 0 ? stripe_corner<T>(c0, a.r0)
+                            : (left ? left[(unsigned long long)kt * K - 1] : Num<T>::big());
+  job.stage = nullptr;
+  TileIn<T> tile;
+  tile.col_init = kt ? a.Q + (unsigned long long)(kt - 1) * a.q_stride + c0 : nullptr;
+  tile.top_row = a.m - 1;
+  PathOut po;
+  po.words = a.words + (unsigned long long)kt * (K / 2) * 64ull;
+  po.track_min = false;
+  const int R = stripe_regs<T>(a.n, s);
+  if (R == RF) {
+    stripe_tile_swath<T, RF>(job, po, tile);
+  } else {
+    switch (R / RQ) {
+#define ODBA_TCASE(K)                                                         \
+  case K:                                                                     \
+    if constexpr (K * RQ < RF) stripe_tile_swath<T, K * RQ>(job, po, tile);   \
+    break;
+      ODBA_TCASE(1)
+      ODBA_TCASE(2)
+      ODBA_TCASE(3)
+      ODBA_TCASE(4)
+      ODBA_TCASE(5)
+      ODBA_TCASE(6)
+      ODBA_TCASE(7)
+#undef ODBA_TCASE
+      default:
+        break;
+    }
+  }
+}
+
+__global__ void stripe_walk_init_kernel(StripeWalk *w, int m, int n) {
+  if (threadIdx.x || blockIdx.x) return;
+  w->r = m - 1;
+  w->c = n - 1;
+  w->h = m;
+  w->cur_t = -1;
+  w->lo = 1;
+  w->hi = 0;
+  w->state = 0;
+  w->nt = 0;
+}
+
+// Continues the backtrack through swath s (updateCentroid's loop,
+// dba.hpp:393-421, as in backtrack_kernel) until it leaves the swath to the
+// left or reaches the start cell.  One warp: every lane holds the move word of
+// one of the 32 rows at and below the current cell (the word of the lane that
+// owns the current column), so the walk advances by shuffles and reloads the
+// window only when it leaves those 32 rows or that owner's columns.  Every
+// lane keeps the same walk state; lane 0 does the stores.
+template <typename T>
+__global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
+  const int lane = threadIdx.x & 31;
+  if (blockIdx.x) return;
+  StripeWalk w = *a.walk;
+  if (w.state) return;
+  constexpr int W = 32 * PathTune<T>::RF;
+  const int c0 = s * W, R = stripe_regs<T>(a.n, s);
+  const int os = a.r0;
+  const long long max_cells = (long long)a.m + a.n - 1;
+  int2 *rg = a.ranges;
+  int32_t *tri = a.triples;
+  const bool lead = lane == 0;
+  auto contribute = [&](int rr, int cc) {
+    if (cc != w.cur_t) {
+      if (lead && w.cur_t >= 0 && w.hi >= w.lo) rg[w.cur_t] = make_int2(w.lo, w.hi);
+      w.cur_t = cc;
+      w.lo = rr;
+      w.hi = rr;
+    } else {
+      w.lo = rr;
+    }
+  };
+  auto emit = [&](int mv) {
+    if (lead && tri) {
+      tri[3 * w.nt] = w.r;
+      tri[3 * w.nt + 1] = w.c;
+      tri[3 * w.nt + 2] = mv;
+    }
+    ++w.nt;
+  };
+  bool swath_done = false;
+  while (!swath_done && w.state == 0) {
+    // window: rows w.r - lane, columns of the owner lane of w.c
+    const int top = w.r, owner = (w.c - c0) / R, cbeg = c0 + owner * R;
+    unsigned long long word = 0;
+    const int my_row = top - lane;
+    if (my_row >= 1) {
+      const int rr = my_row - a.r0;
+      const unsigned long long t = (unsigned long long)owner + (rr >> 1);
+      word = a.words[(t * 32 + owner) * 2 + (rr & 1)];
+    }
+    for (;;) {
+      int mv;
+      const unsigned long long wv = __shfl_sync(kFull, word, (top - w.r) & 31);
+      if (w.r == 0) {
+        mv = w.c == 0 ? (os ? kMoveNilOpenRight : kMaxMoveNil) : (os ? kMoveOpenRight : kMoveRight);
+      } else {
+        mv = int((wv >> (2 * (w.c - cbeg))) & 3ull);
+      }
+      if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {
+        // the start cell (dba.hpp:412-415)
+        if (mv != kMoveNilOpenRight) contribute(0, 0);
+        if (lead && w.cur_t >= 0 && w.hi >= w.lo) rg[w.cur_t] = make_int2(w.lo, w.hi);
+        emit(mv);
+        if (lead && a.triple_count) *a.triple_count = w.nt;
+        w.state = 1;
+        break;
+      }
+      if (w.nt >= max_cells - 1) {
+        w.state = 2;
+        break;
+      }
+      emit(mv);
+      if (mv != kMoveOpenRight) contribute(w.r, w.c);
+      if (mv == kMoveDiag) {
+        --w.r;
+        --w.c;
+      } else if (mv == kMoveUp) {
+        --w.r;
+      } else {
+        --w.c;
+      }
+      if (w.r < 0 || w.c < 0) {
+        w.state = 2;
+        break;
+      }
+      if (w.c < c0) {
+        w.h = w.r + 1;
+        swath_done = true;
+        break;
+      }
+      if (top - w.r >= 32 || w.c < cbeg) break;  // reload the window
+    }
+  }
+  if (lead) {
+    if (w.state == 2 && a.triple_count) *a.triple_count = -1;
+    *a.walk = w;
+  }
+}
+
+template <typename T>
+int stripe_grid() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && cached[dev]) return cached[dev];
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, stripe_forward_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>, kRoundWarps * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int g = sms * per_sm;
+  if (dev < 64) cached[dev] = g;
+  return g;
+}
+
+struct StripeLayout {
+  RoundLayout round;
+  size_t off_head, off_prog, off_E, off_Q, off_W, total;
+  unsigned long long e_stride, q_stride;
+  int swaths_max;
+};
+
+template <typename T>
+StripeLayout stripe_layout(const uint64_t *h_lens, int n, uint64_t Lc, int os, int shift) {
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  constexpr int W = 32 * PathTune<T>::RF;
+  uint64_t maxm = 1;
+  for (int k = 0; k < n; ++k) maxm = h_lens[k] > maxm ? h_lens[k] : maxm;
+  StripeLayout S;
+  S.round = round_layout<T>(n, 1, 0, (unsigned long long)n * Lc, 1);
+  S.swaths_max = int((Lc + W - 1) / W);
+  S.e_stride = (maxm + 64 + 31) / 32 * 32;
+  S.q_stride = (unsigned long long)S.swaths_max * W;
+  const unsigned long long K = 1ull << shift;
+  const unsigned long long nq = (maxm - (os ? 1 : 0)) / K + 1;
+  const unsigned long long steps = (maxm + 1) / 2 + 32;
+  size_t o = S.round.total;
+  S.off_head = o; o += 256;
+  S.off_prog = o; o += up(size_t(S.swaths_max) * 8);
+  S.off_E = o; o += up(size_t(S.swaths_max > 1 ? S.swaths_max - 1 : 1) * S.e_stride * sizeof(T));
+  S.off_Q = o; o += up(size_t(nq) * S.q_stride * sizeof(T));
+  S.off_W = o; o += up(size_t(steps) * 64 * 8);
+  S.total = o;
+  return S;
+}
+
+int stripe_shift(int ckpt_rows) {
+  if (ckpt_rows == 0) return 12;  // 4096 rows per tile
+  if (ckpt_rows < 2 || (ckpt_rows & (ckpt_rows - 1))) return -1;
+  int sh = 0;
+  while ((1 << sh) < ckpt_rows) ++sh;
+  return sh;
+}
+
+}  // namespace
+
+template <typename T>
+size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os,
+                                        int ckpt_rows) {
+  const int sh = stripe_shift(ckpt_rows);
+  if (sh < 0 || n < 1 || Lc == 0) return 0;
+  return stripe_layout<T>(h_lens, n, Lc, os, sh).total;
+}
+
+template <typename T>
+int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
+                            const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                            int n, int os, int oe, int ckpt_rows, T *mean, uint32_t *counts,
+                            double *delta, int32_t *triples, int64_t *triple_counts, void *ws,
+                            size_t ws_bytes, cudaStream_t stream) {
+  if (oe)
+    return fail(ODBA_ERR_INVALID_ARGUMENT,
+                "stripe mode supports global and open-start alignment (an open end needs the full path)");
+  const int sh = stripe_shift(ckpt_rows);
+  if (sh < 0) return fail(ODBA_ERR_INVALID_ARGUMENT, "checkpoint rows must be a power of two >= 2 (0: default)");
+  const StripeLayout S = stripe_layout<T>(h_lens, n, Lc, os, sh);
+  if (ws_bytes < S.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "stripe DBA round workspace too small");
+  const RoundLayout &L = S.round;
+  char *base = static_cast<char *>(ws);
+  int *single = reinterpret_cast<int *>(base + L.off_single);
+  int *mseries = single, *mjob = single + n, *d_clen = single + 2 * n, *d_flags = single + 2 * n + 1,
+      *d_mbeg = single + 2 * n + 2, *d_mend = single + 2 * n + 3;
+  unsigned long long *d_coff =
+      reinterpret_cast<unsigned long long *>(base + L.off_single + ((size_t(2 * n + 4) * 4 + 7) / 8) * 8);
+  const int flags = (os ? 1 : 0) | 4;
+  single_job_kernel<<<(n + 255) / 256, 256, 0, stream>>>(mseries, mjob, n, d_clen, int(Lc), d_flags,
+                                                        flags, d_mbeg, d_mend, d_coff);
+  RoundArgs<T> a;
+  a.centroids = centroid;
+  a.coff = d_coff;
+  a.clen = d_clen;
+  a.jflags = d_flags;
+  a.mbeg = d_mbeg;
+  a.mend = d_mend;
+  a.njobs = 1;
+  a.series = series;
+  a.offsets = offsets;
+  a.lens = lens;
+  a.mseries = mseries;
+  a.mjob = mjob;
+  a.order = nullptr;
+  a.nmem = n;
+  a.means = mean;
+  a.counts = counts;
+  a.deltas = delta;
+  a.triples = triples;
+  a.triple_counts = triple_counts;
+  a.counter = reinterpret_cast<unsigned long long *>(base + L.off_counter);
+  a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
+  a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
+  a.rng_off = reinterpret_cast<unsigned long long *>(base + L.off_rng);
+  a.shortcut = reinterpret_cast<int *>(base + L.off_short);
+  a.ranges = reinterpret_cast<int2 *>(base + L.off_ranges);
+  a.edges = reinterpret_cast<T *>(base + L.off_edges);
+  a.edge_stride = L.edge_stride;
+  a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
+  const unsigned long long nr = (unsigned long long)n * Lc;
+  plan_kernel<T><<<1, 32, 0, stream>>>(a);
+  fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
+  if (int rc = check_launch("stripe DBA round set-up")) return rc;
+
+  constexpr int W = 32 * PathTune<T>::RF;
+  char *head = base + S.off_head;
+  StripeArgs<T> sa;
+  sa.series = series;
+  sa.offsets = offsets;
+  sa.y = centroid;
+  sa.n = int(Lc);
+  sa.r0 = os ? 1 : 0;
+  sa.shift = sh;
+  sa.E = reinterpret_cast<T *>(base + S.off_E);
+  sa.e_stride = S.e_stride;
+  sa.Q = reinterpret_cast<T *>(base + S.off_Q);
+  sa.q_stride = S.q_stride;
+  sa.prog = reinterpret_cast<unsigned long long *>(base + S.off_prog);
+  sa.counter = reinterpret_cast<unsigned long long *>(head);
+  sa.err = reinterpret_cast<unsigned *>(head + 8);
+  sa.walk = reinterpret_cast<StripeWalk *>(head + 64);
+  sa.words = reinterpret_cast<unsigned long long *>(base + S.off_W);
+  sa.limit_ns = kWaitLimitNs;
+  const int swaths = int((Lc + W - 1) / W);
+  sa.swaths = swaths;
+  const int K = 1 << sh;
+  unsigned long long trip = 0;
+  for (int k = 0; k < n; ++k) {
+    const int m = int(h_lens[k]);
+    sa.member = k;
+    sa.m = m;
+    sa.ranges = a.ranges + (unsigned long long)k * Lc;
+    sa.triples = triples ? triples + 3ull * trip : nullptr;
+    sa.triple_count = triple_counts ? triple_counts + k : nullptr;
+    trip += (unsigned long long)m + Lc + 1;
+    cudaMemsetAsync(head, 0, 64, stream);
+    cudaMemsetAsync(sa.prog, 0, size_t(swaths) * 8, stream);
+    stripe_walk_init_kernel<<<1, 32, 0, stream>>>(sa.walk, m, int(Lc));
+    const int fgrid = swaths < stripe_grid<T>() * kRoundWarps ? (swaths + kRoundWarps - 1) / kRoundWarps
+                                                              : stripe_grid<T>();
+    stripe_forward_kernel<T, PathTune<T>::RF, PathTune<T>::RQ><<<fgrid, kRoundWarps * 32, 0, stream>>>(sa);
+    const int tiles = (m - sa.r0 + K - 1) / K;
+    const int tgrid = ((tiles > 1 ? tiles : 1) + kRoundWarps - 1) / kRoundWarps;
+    for (int sw = swaths - 1; sw >= 0; --sw) {
+      stripe_tile_kernel<T, PathTune<T>::RF, PathTune<T>::RQ><<<tgrid, kRoundWarps * 32, 0, stream>>>(sa, sw);
+      stripe_walk_kernel<T><<<1, 32, 0, stream>>>(sa, sw);
+    }
+    if (int rc = check_launch("stripe DBA round member kernels")) return rc;
+  }
+  dim3 rg((unsigned(Lc) + 255) / 256, 1);
+  reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
+  return check_launch("stripe DBA round reduce");
+}
+
+template size_t dba_round_stripe_workspace_bytes<float>(const uint64_t *, int, uint64_t, int, int);
+template size_t dba_round_stripe_workspace_bytes<double>(const uint64_t *, int, uint64_t, int, int);
+template int dba_round_stripe_launch<float>(const float *, uint64_t, const float *, const uint64_t *,
+                                            const uint64_t *, const uint64_t *, int, int, int, int,
+                                            float *, uint32_t *, double *, int32_t *, int64_t *,
+                                            void *, size_t, cudaStream_t);
+template int dba_round_stripe_launch<double>(const double *, uint64_t, const double *,
+                                             const uint64_t *, const uint64_t *, const uint64_t *,
+                                             int, int, int, int, double *, uint32_t *, double *,
+                                             int32_t *, int64_t *, void *, size_t, cudaStream_t);
 
 template size_t dba_round_workspace_bytes<float>(const uint64_t *, int, uint64_t, int, int);
 template size_t dba_round_workspace_bytes<double>(const uint64_t *, int, uint64_t, int, int);

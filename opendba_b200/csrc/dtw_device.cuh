@@ -164,11 +164,24 @@ struct NoGate {
 };
 constexpr int kPublishSteps = 64;  // lane 31 publishes every 64 steps (128 rows)
 
+// Row checkpoints (the stripe-mode forward pass): the full cost row
+// r = r0 + k*K - 1 (k >= 1, K = 2^shift >= 2) of this swath's columns is
+// stored at q + (k - 1) * stride + (c - c0) -- q points at this swath's first
+// column.  K is even, so these rows are always the second row of a lane's
+// step pair.
+template <typename T>
+struct CkptOut {
+  T *q;
+  unsigned long long stride;
+  int shift;
+};
+
 // Sweeps one swath.  On return col[] holds, per lane, the costs of the last
 // row m-1 at the lane's columns.  Swath-edge buffers are indexed by r - r0,
 // two rows per 8/16-byte access.
-template <typename T, int R, typename Gate = NoGate>
-__device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R], Gate gate = Gate()) {
+template <typename T, int R, typename Gate = NoGate, bool CKPT = false>
+__device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R], Gate gate = Gate(),
+                                            CkptOut<T> ckpt = CkptOut<T>{nullptr, 0, 1}) {
   using V2 = typename Pair2<T>::V;
   const int lane = threadIdx.x & 31;
   const int m = job.m;
@@ -214,6 +227,15 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
     }
   };
 
+  auto store_ckpt = [&](int ra) {
+    const int kk = ra - r0 + 2;
+    if ((kk & ((1 << ckpt.shift) - 1)) == 0) {
+      T *dst = ckpt.q + (unsigned long long)((kk >> ckpt.shift) - 1) * ckpt.stride + lane * R;
+#pragma unroll
+      for (int j = 0; j < R; ++j) dst[j] = col[j];
+    }
+  };
+
   auto masked_step = [&](int t) {
     const int ra = r0 + 2 * (t - lane);
     T xa = __shfl_up_sync(kFull, xa_cur, 1);
@@ -232,6 +254,7 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
       if (act_a) job.edge_out[ra - r0] = a_last;
       if (act_b) job.edge_out[ra + 1 - r0] = col[R - 1];
     }
+    if (CKPT && act_b) store_ckpt(ra);
   };
 
   // chunk c of lane 0's rows (k = ra - r0 in [64c, 64c + 64)) into slot c % 2;
@@ -317,6 +340,7 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
                                        false);
       xa_cur = xa;
       xb_cur = xb;
+      if (CKPT) store_ckpt(r0 + 2 * (t - lane));
       if (lane31 && has_out) {
         V2 v;
         v.x = a_last;

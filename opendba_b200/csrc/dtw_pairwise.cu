@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "dtw_device.cuh"
+#include "dtw_pipe.cuh"
 #include "odba_internal.h"
 
 namespace odba {
@@ -407,57 +408,6 @@ int whole_pairlist_launch(const T *series, const uint64_t *offsets, const uint64
 // quickly with the pairs it touched written as NaN.
 namespace odba {
 namespace {
-
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
-
-__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long *p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_gpu(unsigned long long *p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long global_timer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-struct PipeGate {
-  static constexpr bool kActive = true;
-  const unsigned long long *prog_in;  // progress word of the previous swath
-  unsigned long long *prog_out;       // progress word of this swath
-  unsigned *err;
-  unsigned long long limit_ns;
-  int avail;                          // input rows known to be published
-
-  __device__ __forceinline__ void wait_in(int k) {
-    if (k <= avail) return;
-    unsigned long long t0 = 0;
-    for (unsigned it = 0;; ++it) {
-      const unsigned long long v = ld_acquire_gpu(prog_in);
-      if (v >= (unsigned long long)k) {
-        avail = int(v);
-        return;
-      }
-      if (*reinterpret_cast<volatile unsigned *>(err)) {
-        avail = 0x7fffffff;
-        return;
-      }
-      const unsigned long long now = global_timer_ns();
-      if (it == 0) {
-        t0 = now;
-      } else if (now - t0 > limit_ns) {
-        atomicExch(err, 1u);
-        avail = 0x7fffffff;
-        return;
-      }
-      __nanosleep(128);
-    }
-  }
-  __device__ __forceinline__ void publish(int k) { st_release_gpu(prog_out, (unsigned long long)k); }
-};
 
 template <typename T>
 struct PipeArgs {

@@ -70,12 +70,24 @@ struct PathOut {
   bool track_min;             // record min / top of this swath's right-edge column
 };
 
+// A tile of a swath (stripe-mode recompute): rows [job.r0, job.m) only, the
+// row below the tile given by col_init (this lane's R columns start at
+// col_init + lane * R), and the open-end top row at top_row (the full
+// matrix's last row).  The default is a whole swath: col_init null (the
+// boundary row) and top_row = job.m - 1.
+template <typename T>
+struct TileIn {
+  const T *col_init;
+  int top_row;
+};
+
 // Sweeps one swath recording moves.  Same wavefront as sweep_swath; in
 // addition lane 31 keeps the minimum of the right-edge column it spills and
 // its top-row value (for the reference's open-end shortcut, dtw.hpp:74-129).
 template <typename T, int R>
 __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const PathOut &po,
-                                                 T (&col)[R], T &edge_min, T &edge_top) {
+                                                 T (&col)[R], T &edge_min, T &edge_top,
+                                                 TileIn<T> tile = TileIn<T>{nullptr, -1}) {
   const int lane = threadIdx.x & 31;
   const int m = job.m;
   const int r0 = job.r0;
@@ -86,15 +98,22 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     for (int j = 0; j < R; ++j) yv[j] = (cl + j < job.n) ? job.y[cl + j] : T(0);
   }
   const T init = r0 ? T(0) : Num<T>::big();
+  if (tile.col_init) {
+    const T *src = tile.col_init + lane * R;
 #pragma unroll
-  for (int j = 0; j < R; ++j) col[j] = init;
+    for (int j = 0; j < R; ++j) col[j] = src[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < R; ++j) col[j] = init;
+  }
+  const int top = tile.top_row >= 0 ? tile.top_row : m - 1;
 
   const bool has_in = job.edge_in != nullptr;
   const bool has_out = job.edge_out != nullptr;
   const int rows = m - r0;
   const int total = (rows + 1) / 2 + 31;
   const bool lane0 = lane == 0, lane31 = lane == 31;
-  const bool oe_top = job.open_end && m >= 2;
+  const bool oe_top = job.open_end && top >= 1;
   const bool fd0 = job.free_diag0 && lane0;
   const int last_x = m - 1, last_e = rows > 0 ? rows - 1 : 0;
   T emin = Num<T>::big(), etop = Num<T>::big();
@@ -117,11 +136,19 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     }
   };
 
-  auto store_words = [&](int t, unsigned long long wa, unsigned long long wb) {
-    ulonglong2 w;
-    w.x = wa;
-    w.y = wb;
-    reinterpret_cast<ulonglong2 *>(po.words)[t * 32 + lane] = w;
+  // rows outside [r0, m) are not stored: in a tile they belong to a
+  // neighbouring tile
+  auto store_words = [&](int t, unsigned long long wa, unsigned long long wb, bool act_a,
+                         bool act_b) {
+    if (act_a && act_b) {
+      ulonglong2 w;
+      w.x = wa;
+      w.y = wb;
+      reinterpret_cast<ulonglong2 *>(po.words)[t * 32 + lane] = w;
+    } else {
+      if (act_a) po.words[(size_t(t) * 32 + lane) * 2] = wa;
+      if (act_b) po.words[(size_t(t) * 32 + lane) * 2 + 1] = wb;
+    }
   };
 
   for (int t = 0; t < total; ++t) {
@@ -141,22 +168,22 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
                                             false, false, wa, wb);
     } else {
       a_last = step_rows2_path<T, R, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
-                                           oe_top && ra == m - 1, oe_top && ra + 1 == m - 1, fd0,
+                                           oe_top && ra == top, oe_top && ra + 1 == top, fd0,
                                            wa, wb);
     }
     xa_cur = xa;
     xb_cur = xb;
-    store_words(t, wa, wb);
+    store_words(t, wa, wb, act_a, act_b);
     if (lane31) {
       if (act_a) {
         if (has_out) job.edge_out[ra - r0] = a_last;
         emin = Num<T>::min2(emin, a_last);
-        if (ra == m - 1) etop = a_last;
+        if (ra == top) etop = a_last;
       }
       if (act_b) {
         if (has_out) job.edge_out[ra + 1 - r0] = col[R - 1];
         emin = Num<T>::min2(emin, col[R - 1]);
-        if (ra + 1 == m - 1) etop = col[R - 1];
+        if (ra + 1 == top) etop = col[R - 1];
       }
     }
   }

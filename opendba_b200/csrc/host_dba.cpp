@@ -72,10 +72,14 @@ struct Ops<float> {
                      int n, int minseg, float *med, void *w, size_t wb, void *st) {
     return odba_segment_blocks_f32(s, o, l, hl, n, minseg, med, w, wb, st);
   }
+  // stripe_rows < 0: full-path round; otherwise stripe mode with that tile height
   static int round(const float *c, uint64_t Lc, const float *s, const uint64_t *o,
                    const uint64_t *l, const uint64_t *hl, int n, int os, int oe, float *mean,
                    uint32_t *cnt, double *delta, int32_t *tri, int64_t *tc, void *w, size_t wb,
-                   void *st) {
+                   void *st, int stripe_rows = -1) {
+    if (stripe_rows >= 0)
+      return odba_dba_round_stripe_f32(c, Lc, s, o, l, hl, n, os, oe, stripe_rows, mean, cnt, delta,
+                                       tri, tc, w, wb, st);
     return odba_dba_round_f32(c, Lc, s, o, l, hl, n, os, oe, mean, cnt, delta, tri, tc, w, wb, st);
   }
 };
@@ -93,13 +97,42 @@ struct Ops<double> {
                      int n, int minseg, double *med, void *w, size_t wb, void *st) {
     return odba_segment_blocks_f64(s, o, l, hl, n, minseg, med, w, wb, st);
   }
+  // stripe_rows < 0: full-path round; otherwise stripe mode with that tile height
   static int round(const double *c, uint64_t Lc, const double *s, const uint64_t *o,
                    const uint64_t *l, const uint64_t *hl, int n, int os, int oe, double *mean,
                    uint32_t *cnt, double *delta, int32_t *tri, int64_t *tc, void *w, size_t wb,
-                   void *st) {
+                   void *st, int stripe_rows = -1) {
+    if (stripe_rows >= 0)
+      return odba_dba_round_stripe_f64(c, Lc, s, o, l, hl, n, os, oe, stripe_rows, mean, cnt, delta,
+                                       tri, tc, w, wb, st);
     return odba_dba_round_f64(c, Lc, s, o, l, hl, n, os, oe, mean, cnt, delta, tri, tc, w, wb, st);
   }
 };
+
+// Full path or stripe mode for a DBA round.  Like the reference
+// (dba.hpp:515-527), stripe mode is chosen when the full-path workspace does
+// not fit in free device memory; ODBA_FORCE_STRIPE=1 forces it.  Stripe mode
+// covers global and open-start alignment; with an open end the full path is
+// always used.  Returns the workspace bytes; *stripe_rows is -1 (full path)
+// or the stripe tile height (0 = the library default).
+template <typename T>
+size_t round_workspace(const uint64_t *lens, int n, uint64_t Lc, int os, int oe, int *stripe_rows) {
+  const size_t full = odba_dba_round_workspace_bytes(sizeof(T), lens, n, Lc, os, oe);
+  *stripe_rows = -1;
+  if (oe) return full;
+  bool stripe = false;
+  if (const char *f = std::getenv("ODBA_FORCE_STRIPE")) stripe = *f && *f != '0';
+  if (!stripe) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && full > fr / 20 * 19) stripe = true;
+    cudaGetLastError();
+  }
+  if (!stripe) return full;
+  int rows = 0;
+  if (const char *r = std::getenv("ODBA_STRIPE_ROWS")) rows = std::atoi(r);
+  *stripe_rows = rows;
+  return odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, rows);
+}
 
 // RAII device buffer.
 struct DevBuf {
@@ -415,7 +448,8 @@ std::vector<T> converge_cluster(const DeviceSet<T> &all, const std::vector<int> 
   DevBuf d_moffs(n * sizeof(uint64_t)), d_mlens(n * sizeof(uint64_t));
   check_cuda(cudaMemcpyAsync(d_moffs.p, m_offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "member offsets");
   check_cuda(cudaMemcpyAsync(d_mlens.p, m_lens.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st), "member lengths");
-  DevBuf ws(odba_dba_round_workspace_bytes(sizeof(T), m_lens.data(), n, Lc, os, oe));
+  int stripe_rows = -1;
+  DevBuf ws(round_workspace<T>(m_lens.data(), n, Lc, os, oe, &stripe_rows));
   DevBuf d_c(Lc * sizeof(T)), d_mean(Lc * sizeof(T)), d_counts(Lc * sizeof(uint32_t)),
       d_delta(sizeof(double));
   size_t cap = 0;
@@ -430,7 +464,7 @@ std::vector<T> converge_cluster(const DeviceSet<T> &all, const std::vector<int> 
     check(Ops<T>::round(ptr<T>(d_c), Lc, ptr<T>(all.data), ptr<uint64_t>(d_moffs),
                         ptr<uint64_t>(d_mlens), m_lens.data(), n, os, oe, ptr<T>(d_mean),
                         ptr<uint32_t>(d_counts), ptr<double>(d_delta), ptr<int32_t>(d_tri),
-                        ptr<int64_t>(d_tc), ws.p, ws.bytes, st),
+                        ptr<int64_t>(d_tc), ws.p, ws.bytes, st, stripe_rows),
           "DBA round");
     double delta = 0;
     check_cuda(cudaMemcpyAsync(nb.data(), d_mean.p, Lc * sizeof(T), cudaMemcpyDeviceToHost, st), "centroid download");
@@ -536,8 +570,9 @@ double DBAUpdate(T *C, size_t centerLength, T **sequences, char **sequence_names
   DeviceSet<T> ds;
   ds.upload(sequences, sequence_lengths, n, stream);
   std::vector<T> centroid = fetch_series(C, centerLength);
-  DevBuf ws(odba_dba_round_workspace_bytes(sizeof(T), ds.h_lens.data(), n, centerLength,
-                                           use_open_start, use_open_end));
+  int stripe_rows = -1;
+  DevBuf ws(round_workspace<T>(ds.h_lens.data(), n, centerLength, use_open_start, use_open_end,
+                               &stripe_rows));
   DevBuf d_c(centerLength * sizeof(T)), d_mean(centerLength * sizeof(T)),
       d_counts(centerLength * sizeof(uint32_t)), d_delta(sizeof(double));
   size_t cap = 0;
@@ -547,7 +582,8 @@ double DBAUpdate(T *C, size_t centerLength, T **sequences, char **sequence_names
   check(Ops<T>::round(ptr<T>(d_c), centerLength, ptr<T>(ds.data), ptr<uint64_t>(ds.offs),
                       ptr<uint64_t>(ds.lens), ds.h_lens.data(), n, use_open_start, use_open_end,
                       ptr<T>(d_mean), ptr<uint32_t>(d_counts), ptr<double>(d_delta),
-                      ptr<int32_t>(d_tri), ptr<int64_t>(d_tc), ws.p, ws.bytes, stream),
+                      ptr<int32_t>(d_tri), ptr<int64_t>(d_tc), ws.p, ws.bytes, stream,
+                      stripe_rows),
         "DBA round");
   double delta = 0;
   check_cuda(cudaMemcpyAsync(updatedMean, d_mean.p, centerLength * sizeof(T), cudaMemcpyDefault, stream), "centroid download");
@@ -1370,62 +1406,111 @@ int run_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, co
   check_cuda(cudaMemcpyAsync(d_flags.p, h_flags.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "flags");
   std::vector<T> nb(ctot);
   if (batched && live) {
-    // all flags active for sizing (inactive jobs only skip work)
-    std::vector<int> size_flags(njobs);
-    for (int j = 0; j < njobs; ++j) size_flags[j] = (js.flags[j] & 3) | 4;
-    DevBuf rws(odba_dba_batch_workspace_bytes(sizeof(T), h_mlens.data(), mjob.data(), n, h_clen.data(),
-                                              size_flags.data(), njobs));
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    for (int g = 0; g < 2; ++g) {
-      cudaGraph_t graph;
-      check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
-      const T *cin = ptr<T>(cbuf[g]);
-      T *cout = ptr<T>(cbuf[1 - g]);
-      const int rc = sizeof(T) == 4
-          ? odba_dba_batch_round_f32((const float *)cin, ptr<uint64_t>(d_coff), ptr<int>(d_clen), ptr<int>(d_flags),
-                                     ptr<int>(d_mbeg), ptr<int>(d_mend), njobs, max_clen,
-                                     (const float *)js.ds.data.p, ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens),
-                                     ptr<int>(d_mseries), ptr<int>(d_mjob), ptr<int>(d_order), n, h_mlens.data(),
-                                     mjob.data(), h_clen.data(), size_flags.data(), (float *)cout,
-                                     ptr<uint32_t>(d_counts), ptr<double>(d_deltas), nullptr, nullptr, rws.p,
-                                     rws.bytes, st)
-          : odba_dba_batch_round_f64((const double *)cin, ptr<uint64_t>(d_coff), ptr<int>(d_clen), ptr<int>(d_flags),
-                                     ptr<int>(d_mbeg), ptr<int>(d_mend), njobs, max_clen,
-                                     (const double *)js.ds.data.p, ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens),
-                                     ptr<int>(d_mseries), ptr<int>(d_mjob), ptr<int>(d_order), n, h_mlens.data(),
-                                     mjob.data(), h_clen.data(), size_flags.data(), (double *)cout,
-                                     ptr<uint32_t>(d_counts), ptr<double>(d_deltas), nullptr, nullptr, rws.p,
-                                     rws.bytes, st);
-      check_cuda(cudaStreamEndCapture(st, &graph), "graph capture");
-      check(rc, "batched DBA round (capture)");
-      check_cuda(cudaGraphInstantiate(&exec[g], graph, 0), "graph instantiate");
-      cudaGraphDestroy(graph);
+    // Waves: jobs in order, as many per wave as the round workspace budget
+    // allows (only a wave's jobs are active and take path space); each wave
+    // runs its rounds to convergence from two captured graphs.
+    auto ws_for = [&](const std::vector<int> &fl) {
+      return odba_dba_batch_workspace_bytes(sizeof(T), h_mlens.data(), mjob.data(), n, h_clen.data(),
+                                            fl.data(), njobs);
+    };
+    size_t budget = 0;
+    if (const char *e = std::getenv("ODBA_ROUND_BUDGET_BYTES")) budget = std::strtoull(e, nullptr, 10);
+    if (!budget) {
+      size_t fr = 0, tot = 0;
+      check_cuda(cudaMemGetInfo(&fr, &tot), "device memory query");
+      budget = fr / 10 * 7;
     }
-    int cur = 0;
-    for (int round = 0; round < max_rounds && live; ++round) {
-      check_cuda(cudaMemcpyAsync(d_flags.p, h_flags.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "flags");
-      check_cuda(cudaGraphLaunch(exec[cur], st), "graph launch");
-      check_cuda(cudaMemcpyAsync(nb.data(), cbuf[1 - cur].p, ctot * sizeof(T), cudaMemcpyDeviceToHost, st), "means");
-      check_cuda(cudaMemcpyAsync(deltas.data(), d_deltas.p, njobs * sizeof(double), cudaMemcpyDeviceToHost, st), "deltas");
-      check_cuda(cudaStreamSynchronize(st), "batched round");
+    std::vector<int> none(njobs);
+    for (int j = 0; j < njobs; ++j) none[j] = js.flags[j] & 3;
+    const size_t fixed = ws_for(none);
+    std::vector<std::vector<int>> waves;
+    {
+      std::vector<int> cur_wave, fl = none;
+      size_t used = fixed;
       for (int j = 0; j < njobs; ++j) {
         if (!active[j]) continue;
-        rounds[j] = round + 1;
-        std::vector<T> v(nb.begin() + coff[j], nb.begin() + coff[j] + clen[j]);
-        const bool open = (js.flags[j] & 3) != 0;
-        std::copy(v.begin(), v.end(), host_c.begin() + coff[j]);
-        h_deltas[j] = deltas[j];
-        if (flip_flop_or_done<T>(deltas[j], round, open, v, prev[j], two_prev[j])) {
-          active[j] = 0;
-          --live;
+        fl[j] = none[j] | 4;
+        const size_t cost = ws_for(fl) - fixed;
+        fl[j] = none[j];
+        if (!cur_wave.empty() && used + cost > budget) {
+          waves.push_back(cur_wave);
+          cur_wave.clear();
+          used = fixed;
         }
+        cur_wave.push_back(j);
+        used += cost;
+      }
+      if (!cur_wave.empty()) waves.push_back(cur_wave);
+    }
+    size_t ws_max = fixed;
+    for (auto &w : waves) {
+      std::vector<int> fl = none;
+      for (int j : w) fl[j] |= 4;
+      ws_max = std::max(ws_max, ws_for(fl));
+    }
+    DevBuf rws(ws_max);
+    const std::vector<int> was_active = active;
+    for (auto &wave : waves) {
+      std::vector<int> size_flags = none;
+      for (int j = 0; j < njobs; ++j) active[j] = 0;
+      live = 0;
+      for (int j : wave) {
+        size_flags[j] |= 4;
+        active[j] = was_active[j];
+        live += active[j];
       }
       flags_now();
-      // the next round reads the means just written: copy finished jobs'
-      // values along so both buffers agree for them
-      cur = 1 - cur;
+      cudaGraphExec_t exec[2] = {nullptr, nullptr};
+      for (int g = 0; g < 2; ++g) {
+        cudaGraph_t graph;
+        check_cuda(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
+        const T *cin = ptr<T>(cbuf[g]);
+        T *cout = ptr<T>(cbuf[1 - g]);
+        const int rc = sizeof(T) == 4
+            ? odba_dba_batch_round_f32((const float *)cin, ptr<uint64_t>(d_coff), ptr<int>(d_clen), ptr<int>(d_flags),
+                                       ptr<int>(d_mbeg), ptr<int>(d_mend), njobs, max_clen,
+                                       (const float *)js.ds.data.p, ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens),
+                                       ptr<int>(d_mseries), ptr<int>(d_mjob), ptr<int>(d_order), n, h_mlens.data(),
+                                       mjob.data(), h_clen.data(), size_flags.data(), (float *)cout,
+                                       ptr<uint32_t>(d_counts), ptr<double>(d_deltas), nullptr, nullptr, rws.p,
+                                       rws.bytes, st)
+            : odba_dba_batch_round_f64((const double *)cin, ptr<uint64_t>(d_coff), ptr<int>(d_clen), ptr<int>(d_flags),
+                                       ptr<int>(d_mbeg), ptr<int>(d_mend), njobs, max_clen,
+                                       (const double *)js.ds.data.p, ptr<uint64_t>(js.ds.offs), ptr<uint64_t>(js.ds.lens),
+                                       ptr<int>(d_mseries), ptr<int>(d_mjob), ptr<int>(d_order), n, h_mlens.data(),
+                                       mjob.data(), h_clen.data(), size_flags.data(), (double *)cout,
+                                       ptr<uint32_t>(d_counts), ptr<double>(d_deltas), nullptr, nullptr, rws.p,
+                                       rws.bytes, st);
+        check_cuda(cudaStreamEndCapture(st, &graph), "graph capture");
+        check(rc, "batched DBA round (capture)");
+        check_cuda(cudaGraphInstantiate(&exec[g], graph, 0), "graph instantiate");
+        cudaGraphDestroy(graph);
+      }
+      int cur = 0;
+      for (int round = 0; round < max_rounds && live; ++round) {
+        check_cuda(cudaMemcpyAsync(d_flags.p, h_flags.data(), njobs * sizeof(int), cudaMemcpyHostToDevice, st), "flags");
+        check_cuda(cudaGraphLaunch(exec[cur], st), "graph launch");
+        check_cuda(cudaMemcpyAsync(nb.data(), cbuf[1 - cur].p, ctot * sizeof(T), cudaMemcpyDeviceToHost, st), "means");
+        check_cuda(cudaMemcpyAsync(deltas.data(), d_deltas.p, njobs * sizeof(double), cudaMemcpyDeviceToHost, st), "deltas");
+        check_cuda(cudaStreamSynchronize(st), "batched round");
+        for (int j = 0; j < njobs; ++j) {
+          if (!active[j]) continue;
+          rounds[j] = round + 1;
+          std::vector<T> v(nb.begin() + coff[j], nb.begin() + coff[j] + clen[j]);
+          const bool open = (js.flags[j] & 3) != 0;
+          std::copy(v.begin(), v.end(), host_c.begin() + coff[j]);
+          h_deltas[j] = deltas[j];
+          if (flip_flop_or_done<T>(deltas[j], round, open, v, prev[j], two_prev[j])) {
+            active[j] = 0;
+            --live;
+          }
+        }
+        flags_now();
+        // the next round reads the means just written (the other buffer)
+        cur = 1 - cur;
+      }
+      for (int g = 0; g < 2; ++g) cudaGraphExecDestroy(exec[g]);
     }
-    for (int g = 0; g < 2; ++g) cudaGraphExecDestroy(exec[g]);
   } else if (live) {
     // plain: job by job, one round per call, synchronizing every round (performDBA's loop)
     for (int j = 0; j < njobs; ++j) {

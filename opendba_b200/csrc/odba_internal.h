@@ -75,6 +75,16 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
                      void *ws, size_t ws_bytes, cudaStream_t stream);
 
 template <typename T>
+size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os,
+                                        int ckpt_rows);
+template <typename T>
+int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
+                            const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                            int n, int os, int oe, int ckpt_rows, T *mean, uint32_t *counts,
+                            double *delta, int32_t *triples, int64_t *triple_counts, void *ws,
+                            size_t ws_bytes, cudaStream_t stream);
+
+template <typename T>
 size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int nmem,
                                  const uint64_t *h_clen, const int *h_flags, int njobs);
 template <typename T>

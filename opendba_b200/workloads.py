@@ -28,10 +28,11 @@ def _step(rng, L):
 
 def make_jobs(n_jobs, count_lo, count_hi, len_lo, len_hi, seed):
     """Independent averaging jobs: per job a log-uniform count of series with
-    log-uniform lengths."""
+    log-uniform lengths (step signals: N(90,12) levels, dwell 10, noise 2)."""
     rng = np.random.default_rng(seed)
     counts = _logu_int(rng, count_lo, count_hi + 1, n_jobs)
-    return [[_step(rng, L) for L in _logu_int(rng, len_lo, len_hi + 1, int(c))] for c in counts]
+    return [synth.step_signals(rng, _logu_int(rng, len_lo, len_hi + 1, int(c)), 90.0, 12.0, 10.0, 2.0)
+            for c in counts]
 
 
 def job_cells(job, rounds, centroid_len):
@@ -41,9 +42,15 @@ def job_cells(job, rounds, centroid_len):
     return pair_cells + rounds * tot * centroid_len
 
 
-def run_batched_vs_plain(n_jobs=48, count_lo=8, count_hi=96, len_lo=200, len_hi=4000,
-                         open_end=1, seed=0x0DBA0004):
-    """Many DBA jobs (open end, float32): batched vs plain; returns a dict."""
+def run_batched_vs_plain(n_jobs=256, count_lo=8, count_hi=512, len_lo=200, len_hi=20000,
+                         open_end=1, seed=synth.SEED_BASE + 3, plain_sample=24):
+    """Many DBA jobs (open end, float32): batched vs plain; returns a dict.
+    Defaults: 256 jobs of 8-512 series (log-uniform count), lengths
+    log-uniform in [200, 20000].  The batched path runs every job; the plain
+    path (one job after another, a synchronisation every round) runs a seeded
+    sample of ``plain_sample`` jobs, whose results must equal the batched
+    ones, and its throughput (cells per second) is measured on that sample."""
+    import sys
     jobs = make_jobs(n_jobs, count_lo, count_hi, len_lo, len_hi, seed)
     flags = [2 if open_end else 0] * len(jobs)
     api.dba_jobs(jobs[:2], flags[:2], norm=1, batched=True)   # warm-up (module loading)
@@ -51,19 +58,26 @@ def run_batched_vs_plain(n_jobs=48, count_lo=8, count_hi=96, len_lo=200, len_hi=
     t0 = time.perf_counter()
     res_b = api.dba_jobs(jobs, flags, norm=1, batched=True)
     tb = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    res_p = api.dba_jobs(jobs, flags, norm=1, batched=False)
-    tp = time.perf_counter() - t0
-    same = all(a["medoid"] == b["medoid"] and a["rounds"] == b["rounds"] and
-               np.array_equal(a["centroid"].view(np.uint32), b["centroid"].view(np.uint32))
-               for a, b in zip(res_b, res_p))
     cells = sum(job_cells(j, r["rounds"], len(r["centroid"])) for j, r in zip(jobs, res_b))
+    print(f"batched: {len(jobs)} jobs, {cells:.3e} cells in {tb:.1f} s", file=sys.stderr, flush=True)
+    rng = np.random.default_rng(seed + 1)
+    pick = sorted(rng.choice(len(jobs), size=min(plain_sample, len(jobs)), replace=False).tolist())
+    t0 = time.perf_counter()
+    res_p = api.dba_jobs([jobs[i] for i in pick], [flags[i] for i in pick], norm=1, batched=False)
+    tp = time.perf_counter() - t0
+    pcells = sum(job_cells(jobs[i], r["rounds"], len(r["centroid"])) for i, r in zip(pick, res_p))
+    print(f"plain: {len(pick)} jobs, {pcells:.3e} cells in {tp:.1f} s", file=sys.stderr, flush=True)
+    same = all(res_b[i]["medoid"] == b["medoid"] and res_b[i]["rounds"] == b["rounds"] and
+               np.array_equal(res_b[i]["centroid"].view(np.uint32), b["centroid"].view(np.uint32))
+               for i, b in zip(pick, res_p))
+    bg, pg = cells / tb / 1e9, pcells / tp / 1e9
     return {"workload": f"{len(jobs)} DBA jobs of {count_lo}-{count_hi} series (log-uniform), lengths "
                         f"log-uniform [{len_lo},{len_hi}], open end, float32, z-normalised",
-            "cells": cells, "batched_s": tb, "plain_s": tp,
-            "batched_gcups": cells / tb / 1e9, "plain_gcups": cells / tp / 1e9,
-            "speedup": tp / tb, "identical_results": bool(same),
-            "rounds_mean": float(np.mean([r["rounds"] for r in res_b]))}
+            "cells": cells, "batched_s": tb, "batched_gcups": bg,
+            "plain_sample_jobs": len(pick), "plain_sample_cells": pcells, "plain_sample_s": tp,
+            "plain_gcups": pg, "speedup": bg / pg, "identical_results_on_sample": bool(same),
+            "rounds_mean": float(np.mean([r["rounds"] for r in res_b])),
+            "rounds_max": int(max(r["rounds"] for r in res_b))}
 
 
 def make_requests(n, seed, n_centroids=32, centroid_len=4000, query_frac=0.7,

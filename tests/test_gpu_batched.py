@@ -77,3 +77,20 @@ def test_batched_jobs_equal_plain_and_oracle(api, dtype):
         assert np.array_equal(_bits(b["centroid"]), _bits(r["centroid"])), j
         if len(jobs[j]) > 1:
             assert b["rounds"] == r["rounds"], j
+
+
+def test_batched_rounds_in_memory_bounded_waves(api, monkeypatch):
+    # a tiny round budget forces one job per wave; results must not change
+    rng = np.random.default_rng(77)
+    jobs = [[(np.cumsum(rng.standard_normal(int(L))) + 30.0).astype(np.float32)
+             for L in rng.integers(50, 900, size=int(k))] for k in (6, 2, 9, 4, 7)]
+    flags = [0, 2, 2, 1, 0]
+    whole = api.dba_jobs(jobs, flags, norm=1, batched=True)
+    monkeypatch.setenv("ODBA_ROUND_BUDGET_BYTES", "1")
+    waves = api.dba_jobs(jobs, flags, norm=1, batched=True)
+    plain = api.dba_jobs(jobs, flags, norm=1, batched=False)
+    for a, b, c in zip(whole, waves, plain):
+        assert a["medoid"] == b["medoid"] == c["medoid"]
+        assert a["rounds"] == b["rounds"] == c["rounds"]
+        assert np.array_equal(_bits(a["centroid"]), _bits(b["centroid"]))
+        assert np.array_equal(_bits(a["centroid"]), _bits(c["centroid"]))
