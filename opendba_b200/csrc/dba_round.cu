@@ -145,10 +145,11 @@ __device__ __forceinline__ void path_swath(const SwathJob<T> &job, const PathOut
   sweep_swath_path<T, R>(job, po, col, emin, etop);
 }
 
-template <typename T, int RF, int RQ>
+template <typename T, int RF, int RQ, int WARPS>
 __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T> a) {
+  __shared__ __align__(16) T stage_mem[WARPS * kStageElems];
   const int lane = threadIdx.x & 31;
-  const long long slot = (long long)blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
+  const long long slot = (long long)blockIdx.x * WARPS + (threadIdx.x >> 5);
   T *e0 = a.edges + slot * 2 * a.edge_stride;
   T *e1 = e0 + a.edge_stride;
   constexpr int W = 32 * RF;
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
     job.n = g.n;
     job.r0 = g.r0;
     job.open_end = oe != 0;
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     int shortcut = 0;
     const bool check_short = oe && !os;
     for (int s = 0; s < g.swaths; ++s) {
@@ -222,65 +224,43 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
   }
 }
 
-// Decodes the reference's move at (r, c) of member geometry g.
+// The backtrack (updateCentroid's loop, dba.hpp:374-423): one warp per
+// member walks its path from the end cell back to (0, 0).  Every lane holds
+// the move word of one of the 32 rows at and below the current cell (the
+// word of the lane that owned the current column in the path sweep), so the
+// walk advances by shuffles and reloads only when it leaves those 32 rows or
+// that owner's columns -- about once per 32 steps instead of one dependent
+// global load per step.  Every lane keeps the same walk state; lane 0 stores
+// the per-centroid-index sample ranges and, if asked, the path listing.
+// Moves are decoded as the reference defines them: the open-end shortcut
+// overrides the top row first (with a single-row matrix that row is row 0,
+// dtw.hpp:105-108 runs before the row-0 loop), then row 0 (RIGHT or
+// OPEN_RIGHT, NIL / NIL_OPEN_RIGHT at (0, 0)), then the recorded code with
+// RIGHT on the open-end top row meaning OPEN_RIGHT.
 template <typename T>
-__device__ __forceinline__ int move_at(const MemberGeom &g, int os, int oe,
-                                       const unsigned long long *w, int shortcut, int r, int c,
-                                       unsigned long long &cache_idx,
-                                       unsigned long long &cache_word) {
-  // the shortcut overrides the top row first: with a single-row matrix that
-  // row is row 0 (dtw.hpp:105-108 runs before the row-0 loop)
-  if (shortcut && r == g.m - 1 && c >= shortcut) return kMoveOpenRight;
-  if (r == 0) {
-    if (c == 0) return os ? kMoveNilOpenRight : kMaxMoveNil;
-    return os ? kMoveOpenRight : kMoveRight;
-  }
-  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
-  const int s = c / W;
-  const int c0 = s * W;
-  int R = RF;
-  if (s == g.swaths - 1) {
-    const int width = g.n - c0;
-    const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
-    R = rq < RF ? rq : RF;
-  }
-  const int cl = c - c0;
-  const int lane = cl / R, j = cl - lane * R;
-  const int rr = r - g.r0;
-  const int t = lane + (rr >> 1);
-  const unsigned long long idx =
-      (unsigned long long)s * g.steps * 64ull + ((unsigned long long)t * 32 + lane) * 2 + (rr & 1);
-  if (idx != cache_idx) {
-    cache_word = w[idx];
-    cache_idx = idx;
-  }
-  const int code = int((cache_word >> (2 * j)) & 3ull);
-  if (code == kMoveRight && oe && r == g.m - 1) return kMoveOpenRight;
-  return code;
-}
-
-template <typename T>
-__global__ void backtrack_kernel(RoundArgs<T> a) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
   if (k >= a.nmem) return;
   int jb;
   const MemberGeom g = geom_of<T>(a, k, jb);
   const int flags = a.jflags[jb];
   if (!(flags & 4)) return;
   const int os = flags & 1, oe = (flags >> 1) & 1;
+  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
   int2 *rg = a.ranges + a.rng_off[k];
   int32_t *tri = a.triples ? a.triples + 3ull * a.trip_off[k] : nullptr;
+  const bool lead = lane == 0;
   long long nt = 0;
   int r = g.m - 1, c = g.n - 1;
-  unsigned long long cache_idx = ~0ull, cache_word = 0;
   int cur_t = -1, lo = 1, hi = 0;
   auto contribute = [&](int rr, int cc) {
-    const int ti = g.flip ? rr : cc;     // centroid index
-    const int mi = g.flip ? cc : rr;     // member sample index
+    const int ti = g.flip ? rr : cc;  // centroid index
+    const int mi = g.flip ? cc : rr;  // member sample index
     if (ti != cur_t) {
-      if (cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
+      if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
       cur_t = ti;
       lo = mi;
       hi = mi;
@@ -288,47 +268,75 @@ __global__ void backtrack_kernel(RoundArgs<T> a) {
       lo = mi;  // the walk only moves toward smaller indices
     }
   };
-  int mv = move_at<T>(g, os, oe, w, shortcut, r, c, cache_idx, cache_word);
-  // A path has at most m + n - 1 cells and never leaves the matrix; the checks
-  // only keep a corrupt path buffer from turning into an endless or
-  // out-of-bounds walk (the member is then reported with a count of -1).
-  const long long max_cells = (long long)g.m + g.n - 1;
-  while (mv != kMaxMoveNil && mv != kMoveNilOpenRight) {
-    if (nt >= max_cells - 1) {
-      if (a.triple_counts) a.triple_counts[k] = -1;
-      return;
-    }
-    if (tri) {
+  auto emit = [&](int mv) {
+    if (lead && tri) {
       tri[3 * nt] = r;
       tri[3 * nt + 1] = c;
       tri[3 * nt + 2] = mv;
     }
     ++nt;
-    if (mv != kMoveOpenRight) contribute(r, c);
-    if (mv == kMoveDiag) {
-      --r;
-      --c;
-    } else if (mv == kMoveUp) {
-      --r;
-    } else {
-      --c;
+  };
+  // A path has at most m + n - 1 cells and never leaves the matrix; the checks
+  // only keep a corrupt path buffer from turning into an endless or
+  // out-of-bounds walk (the member is then reported with a count of -1).
+  const long long max_cells = (long long)g.m + g.n - 1;
+  bool failed = false, done = false;
+  while (!done && !failed) {
+    const int s = c / W, c0 = s * W;
+    int R = RF;
+    if (s == g.swaths - 1) {
+      const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
+      R = rq < RF ? rq : RF;
     }
-    if (r < 0 || c < 0) {
-      if (a.triple_counts) a.triple_counts[k] = -1;
-      return;
+    const int top = r, owner = (c - c0) / R, cbeg = c0 + owner * R;
+    unsigned long long word = 0;
+    const int my_row = top - lane;
+    if (my_row >= 1) {
+      const int rr = my_row - g.r0;
+      const unsigned long long t = (unsigned long long)owner + (rr >> 1);
+      word = w[(unsigned long long)s * g.steps * 64ull + (t * 32 + owner) * 2 + (rr & 1)];
     }
-    mv = move_at<T>(g, os, oe, w, shortcut, r, c, cache_idx, cache_word);
+    for (;;) {
+      const unsigned long long wv = __shfl_sync(kFull, word, (top - r) & 31);
+      int mv;
+      if (shortcut && r == g.m - 1 && c >= shortcut) {
+        mv = kMoveOpenRight;
+      } else if (r == 0) {
+        mv = c == 0 ? (os ? kMoveNilOpenRight : kMaxMoveNil) : (os ? kMoveOpenRight : kMoveRight);
+      } else {
+        mv = int((wv >> (2 * (c - cbeg))) & 3ull);
+        if (mv == kMoveRight && oe && r == g.m - 1) mv = kMoveOpenRight;
+      }
+      if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {
+        // the start cell (dba.hpp:412-415)
+        if (mv != kMoveNilOpenRight) contribute(0, 0);
+        if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
+        emit(mv);
+        done = true;
+        break;
+      }
+      if (nt >= max_cells - 1) {
+        failed = true;
+        break;
+      }
+      emit(mv);
+      if (mv != kMoveOpenRight) contribute(r, c);
+      if (mv == kMoveDiag) {
+        --r;
+        --c;
+      } else if (mv == kMoveUp) {
+        --r;
+      } else {
+        --c;
+      }
+      if (r < 0 || c < 0) {
+        failed = true;
+        break;
+      }
+      if (top - r >= 32 || c < cbeg) break;  // reload the window
+    }
   }
-  // the start cell (dba.hpp:412-415)
-  if (mv != kMoveNilOpenRight) contribute(0, 0);
-  if (cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
-  if (tri) {
-    tri[3 * nt] = r;
-    tri[3 * nt + 1] = c;
-    tri[3 * nt + 2] = mv;
-  }
-  ++nt;
-  if (a.triple_counts) a.triple_counts[k] = nt;
+  if (lead && a.triple_counts) a.triple_counts[k] = failed ? -1 : nt;
 }
 
 // The reference divides on the host (dba.hpp:820-822); a centroid index that
@@ -415,7 +423,7 @@ int round_grid() {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>, kRoundWarps * 32, 0);
+      &per_sm, path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, kRoundWarps>, kRoundWarps * 32, 0);
   if (per_sm < 1) per_sm = 1;
   const int g = sms * per_sm;
   if (dev < 64) cached[dev] = g;
@@ -485,9 +493,15 @@ int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen
   cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
   plan_kernel<T><<<1, 32, 0, stream>>>(a);
   fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
-  path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>
-      <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
-  backtrack_kernel<T><<<(a.nmem + 127) / 128, 128, 0, stream>>>(a);
+  // with fewer members than resident warps, one block per member spreads
+  // them over the SMs instead of leaving them to the first blocks placed
+  const bool spread = a.nmem < round_grid<T>() * kRoundWarps;
+  if (spread)
+    path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, 1><<<a.nmem, 32, 0, stream>>>(a);
+  else
+    path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, kRoundWarps>
+        <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
+  backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
   dim3 rg((max_clen + 255) / 256, a.njobs);
   reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
   return check_launch("DBA round kernels");
@@ -733,6 +747,7 @@ __device__ __forceinline__ void stripe_tile_swath(const SwathJob<T> &job, const 
 // One warp per K-row tile of swath s below the backtrack height.
 template <typename T, int RF, int RQ>
 __global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArgs<T> a, int s) {
+  __shared__ __align__(16) T stage_mem[kRoundWarps * kStageElems];
   constexpr int W = 32 * RF;
   const int kt = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
   const int H = a.walk->h;
@@ -756,7 +771,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArg
   job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
   job.corner_init = kt == 0 ? stripe_corner<T>(c0, a.r0)
                             : (left ? left[(unsigned long long)kt * K - 1] : Num<T>::big());
-  job.stage = nullptr;
+  job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
   TileIn<T> tile;
   tile.col_init = kt ? a.Q + (unsigned long long)(kt - 1) * a.q_stride + c0 : nullptr;
   tile.top_row = a.m - 1;

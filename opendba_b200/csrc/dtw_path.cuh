@@ -151,7 +151,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     }
   };
 
-  for (int t = 0; t < total; ++t) {
+  auto masked_step = [&](int t) {
     const int ra = r0 + 2 * (t - lane);
     T xa = __shfl_up_sync(kFull, xa_cur, 1);
     T xb = __shfl_up_sync(kFull, xb_cur, 1);
@@ -162,15 +162,8 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     dg = lb;
     const bool act_a = ra >= r0 && ra < m, act_b = ra + 1 >= r0 && ra + 1 < m;
     unsigned long long wa, wb;
-    const bool interior = (t >= 31) && (2 * t + 1 < rows - 1);
-    if (interior) {
-      a_last = step_rows2_path<T, R, false>(col, yv, xa, xb, la, lb, diag, true, true, false,
-                                            false, false, wa, wb);
-    } else {
-      a_last = step_rows2_path<T, R, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
-                                           oe_top && ra == top, oe_top && ra + 1 == top, fd0,
-                                           wa, wb);
-    }
+    a_last = step_rows2_path<T, R, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
+                                         oe_top && ra == top, oe_top && ra + 1 == top, fd0, wa, wb);
     xa_cur = xa;
     xb_cur = xb;
     store_words(t, wa, wb, act_a, act_b);
@@ -186,7 +179,98 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
         if (ra + 1 == top) etop = col[R - 1];
       }
     }
+  };
+
+  // Steady state as in sweep_swath: lane 0's rows staged in shared memory one
+  // 64-row chunk ahead by the whole warp (cp.async), no masks, no top row.
+  auto issue_chunk = [&](int c) {
+    T *slot = job.stage + (c & 1) * (2 * kChunkRows);
+    const int k = c * kChunkRows + 2 * lane;
+    const int ia = r0 + k < last_x ? r0 + k : last_x;
+    const int ib = r0 + k + 1 < last_x ? r0 + k + 1 : last_x;
+    cp_async_elem(slot + 2 * lane, job.x + ia, sizeof(T));
+    cp_async_elem(slot + 2 * lane + 1, job.x + ib, sizeof(T));
+    if (has_in) {
+      const int ka = k < last_e ? k : last_e, kb = k + 1 < last_e ? k + 1 : last_e;
+      cp_async_elem(slot + kChunkRows + 2 * lane, job.edge_in + ka, sizeof(T));
+      cp_async_elem(slot + kChunkRows + 2 * lane + 1, job.edge_in + kb, sizeof(T));
+    }
+    cp_async_commit();
+  };
+  auto staged = [&](int u, T &xa, T &xb, T &ea, T &eb) {
+    using V2 = typename Pair2<T>::V;
+    const T *slot = job.stage + ((u >> 5) & 1) * (2 * kChunkRows);
+    const int i = 2 * (u & 31);
+    const V2 xv = *reinterpret_cast<const V2 *>(slot + i);
+    xa = xv.x;
+    xb = xv.y;
+    if (has_in) {
+      const V2 ev = *reinterpret_cast<const V2 *>(slot + kChunkRows + i);
+      ea = ev.x;
+      eb = ev.y;
+    } else {
+      ea = eb = Num<T>::big();
+    }
+  };
+
+  int steady_end = (rows - 1) / 2;  // first step at which lane 0's row b reaches the last row
+  if (steady_end < 31) steady_end = 31;
+  const int fill_end = total < 31 ? total : 31;
+  int t = 0;
+  for (; t < fill_end; ++t) masked_step(t);
+  if (t < steady_end) {
+    using V2 = typename Pair2<T>::V;
+    const int cfirst = t >> 5;
+    __syncwarp();
+    issue_chunk(cfirst);
+    issue_chunk(cfirst + 1);
+    cp_async_wait_all();
+    __syncwarp();
+    T pxa = T(0), pxb = T(0), pea = T(0), peb = T(0);
+    if (lane0) staged(t, pxa, pxb, pea, peb);
+    for (; t < steady_end; ++t) {
+      T xa = __shfl_up_sync(kFull, xa_cur, 1);
+      T xb = __shfl_up_sync(kFull, xb_cur, 1);
+      T la = __shfl_up_sync(kFull, a_last, 1);
+      T lb = __shfl_up_sync(kFull, col[R - 1], 1);
+      if (((t + 1) & 31) == 0) {
+        cp_async_wait_all();
+        __syncwarp();
+        issue_chunk(((t + 1) >> 5) + 1);
+      }
+      if (lane0) {
+        xa = pxa;
+        xb = pxb;
+        la = pea;
+        lb = peb;
+        staged(t + 1, pxa, pxb, pea, peb);
+      }
+      const T diag = dg;
+      dg = lb;
+      unsigned long long wa, wb;
+      a_last = step_rows2_path<T, R, false>(col, yv, xa, xb, la, lb, diag, true, true, false,
+                                            false, false, wa, wb);
+      xa_cur = xa;
+      xb_cur = xb;
+      ulonglong2 w;
+      w.x = wa;
+      w.y = wb;
+      reinterpret_cast<ulonglong2 *>(po.words)[t * 32 + lane] = w;
+      if (lane31) {
+        if (has_out) {
+          V2 v;
+          v.x = a_last;
+          v.y = col[R - 1];
+          *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
+        }
+        emin = Num<T>::min2(emin, Num<T>::min2(a_last, col[R - 1]));
+      }
+    }
+    // the next swath reuses the slots: no copy may still be in flight
+    cp_async_wait_all();
+    __syncwarp();
   }
+  for (; t < total; ++t) masked_step(t);
   edge_min = __shfl_sync(kFull, emin, 31);
   edge_top = __shfl_sync(kFull, etop, 31);
 }

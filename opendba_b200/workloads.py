@@ -185,7 +185,7 @@ def run_serving(rate_hz, n_requests=60, seed=0x0DBA0005, budget=32 << 30, detail
 
 
 def run_long(n_series=16, len_lo=1_000_000, len_hi=4_000_000, dtypes=("f32", "f64"), minseg=4,
-             seed=0x0DBA0002 + 2):
+             seed=0x0DBA0002 + 2, with_round=True):
     """Few very long series: the k-segmentation DP on each raw series, then
     all-vs-all DTW (global, z-normalised) in float32 and float64, which the
     planner runs as the swath pipeline.  Device time by CUDA events."""
@@ -232,4 +232,36 @@ def run_long(n_series=16, len_lo=1_000_000, len_hi=4_000_000, dtypes=("f32", "f6
                      "finite": bool(np.isfinite(dh).all()), "checksum": float(dh.astype(np.float64).sum())}
         del ds, ws, d
         torch.cuda.empty_cache()
+    if with_round:
+        out["dba_round_stripe"] = _long_round(raw)
     return out
+
+
+def _long_round(raw):
+    """One stripe-mode DBA round (float32, global): all series aligned to the
+    middle-length one as the centroid (the full 2-bit path would need
+    ~sum(len) * len(centroid) / 4 bytes)."""
+    import torch
+    from . import _native
+    ds = api.DeviceSeries.from_host(raw)
+    api.znorm_(ds)
+    mid = len(raw) // 2
+    cen = ds.data[int(ds.offsets[mid]):int(ds.offsets[mid]) + len(raw[mid])].clone()
+    L = np.array([len(s) for s in raw], dtype=np.float64)
+    h = np.ascontiguousarray(ds.host_lens, dtype=np.uint64)
+    lib = _native.lib()
+    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0, 0)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    mean, counts, delta, _ = api.dba_round(cen, ds, 0, 0, workspace=ws, stripe_rows=0)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    cells = float(L.sum()) * len(cen)
+    full_path_tb = float(L.sum()) * len(cen) / 4 / 1e12
+    return {"centroid_len": len(cen), "members": len(raw), "seconds": ms / 1e3,
+            "forward_cells": cells, "gcups": cells / ms / 1e6, "workspace_gb": nbytes / 1e9,
+            "full_path_would_need_tb": full_path_tb, "delta": float(delta),
+            "finite_mean": bool(torch.isfinite(mean).all().item())}
