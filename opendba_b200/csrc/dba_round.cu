@@ -95,6 +95,12 @@ struct RoundArgs {
   T *edges;
   unsigned long long edge_stride;
   unsigned long long *words;
+  // swath pipeline (many warps per member): one progress word and the right
+  // edge's minimum and top-row value per (member, swath)
+  unsigned long long *prog;
+  T *emtop;
+  unsigned *err;
+  int max_swaths;
   T *means;
   uint32_t *counts;
   double *deltas;
@@ -222,6 +228,124 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
     }
     if (lane == 0) a.shortcut[k] = shortcut;
   }
+}
+
+template <typename T, int R>
+__device__ __forceinline__ void path_pipe_swath(const SwathJob<T> &job, const PathOut &po,
+                                                const PipeGate &gate, T &emin, T &etop) {
+  T col[R];
+  sweep_swath_path<T, R, PipeGate>(job, po, col, emin, etop, TileIn<T>{nullptr, -1}, gate);
+}
+
+// Path DTW as the swath pipeline: task k is swath k / nmem of the (k % nmem)-th
+// member in alignment order, so a member's swaths run on different warps at
+// once (few or long members keep the GPU busy); the right edge of swath s goes
+// to buffer s % 2 of the member with one progress word per (member, swath),
+// exactly as in the all-pairs swath pipeline.  Each swath also stores its
+// right edge's minimum and top-row value for the open-end shortcut, which
+// shortcut_kernel resolves afterwards (it never changes a recorded move).
+template <typename T, int RF, int RQ>
+__global__ void __launch_bounds__(kRoundWarps * 32) path_pipe_kernel(RoundArgs<T> a) {
+  __shared__ __align__(16) T stage_mem[kRoundWarps * kStageElems];
+  constexpr int W = 32 * RF;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long ntasks = (unsigned long long)a.nmem * a.max_swaths;
+  for (;;) {
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(a.counter, 1ull);
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= ntasks) break;
+    const int s = int(q / a.nmem), qi = int(q - (unsigned long long)s * a.nmem);
+    const int k = a.order ? a.order[qi] : a.nmem - 1 - qi;
+    int jb;
+    const MemberGeom g = geom_of<T>(a, k, jb);
+    const int flags = a.jflags[jb];
+    if (!(flags & 4) || s >= g.swaths) continue;
+    const int os = flags & 1, oe = (flags >> 1) & 1;
+    const T *seq = a.series + a.offsets[a.mseries[k]];
+    const T *cen = a.centroids + a.coff[jb];
+    T *b0 = a.edges + (unsigned long long)k * 2 * a.edge_stride;
+    T *b1 = b0 + a.edge_stride;
+    const int c0 = s * W;
+    const bool last = s == g.swaths - 1;
+    SwathJob<T> job;
+    job.x = g.flip ? cen : seq;
+    job.y = g.flip ? seq : cen;
+    job.m = g.m;
+    job.n = g.n;
+    job.c0 = c0;
+    job.r0 = g.r0;
+    job.open_end = oe != 0;
+    job.edge_in = s ? (((s - 1) & 1) ? b1 : b0) : nullptr;
+    job.edge_out = last ? nullptr : ((s & 1) ? b1 : b0);
+    job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
+    job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
+    PathOut po;
+    po.words = a.words + a.path_off[k] + (unsigned long long)s * g.steps * 64ull;
+    po.track_min = true;
+    unsigned long long *words = a.prog + (unsigned long long)k * a.max_swaths;
+    PipeGate gate;
+    gate.prog_in = words + (s ? s - 1 : 0);
+    gate.prog_out = words + s;
+    gate.err = a.err;
+    gate.limit_ns = kWaitLimitNs;
+    gate.avail = 0;
+    T emin, etop;
+    const int width = g.n - c0 < W ? g.n - c0 : W;
+    const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
+    if (rq >= RF) {
+      path_pipe_swath<T, RF>(job, po, gate, emin, etop);
+    } else {
+      switch (rq / RQ) {
+#define ODBA_PPCASE(K)                                                                  \
+  case K:                                                                               \
+    if constexpr (K * RQ < RF) path_pipe_swath<T, K * RQ>(job, po, gate, emin, etop);   \
+    break;
+        ODBA_PPCASE(1)
+        ODBA_PPCASE(2)
+        ODBA_PPCASE(3)
+        ODBA_PPCASE(4)
+        ODBA_PPCASE(5)
+        ODBA_PPCASE(6)
+        ODBA_PPCASE(7)
+#undef ODBA_PPCASE
+        default:
+          break;
+      }
+    }
+    if (lane == 0) {
+      T *et = a.emtop + ((unsigned long long)k * a.max_swaths + s) * 2;
+      et[0] = emin;
+      et[1] = etop;
+    }
+  }
+}
+
+// The open-end shortcut of the swath pipeline's members (the rule of
+// path_dtw_kernel, applied to the per-swath right-edge minima afterwards).
+template <typename T>
+__global__ void shortcut_kernel(RoundArgs<T> a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.nmem) return;
+  int jb;
+  const MemberGeom g = geom_of<T>(a, k, jb);
+  const int flags = a.jflags[jb];
+  if (!(flags & 4)) return;
+  const int os = flags & 1, oe = (flags >> 1) & 1;
+  constexpr int W = 32 * PathTune<T>::RF;
+  int shortcut = 0;
+  if (oe && !os) {
+    const T *et = a.emtop + (unsigned long long)k * a.max_swaths * 2;
+    for (int s = 0; s + 1 < g.swaths; ++s) {
+      const int cnext = (s + 1) * W;
+      if (cnext % kRefSwath == 0 && cnext > g.m && cnext < g.n && et[2 * s + 1] == et[2 * s]) {
+        shortcut = cnext;
+        break;
+      }
+    }
+  }
+  a.shortcut[k] = shortcut;
 }
 
 // The backtrack (updateCentroid's loop, dba.hpp:374-423): one warp per
@@ -432,18 +556,25 @@ int round_grid() {
 
 struct RoundLayout {
   size_t off_counter, off_path, off_trip, off_rng, off_short, off_single, off_ranges, off_edges,
-      off_words, total;
+      off_words, off_prog, off_emtop, total;
   unsigned long long edge_stride;
+  int max_swaths;
+  bool pipe;  // path DTW as the swath pipeline (two edge columns per member)
 };
+
+constexpr size_t kPipeEdgeBytes = size_t(8) << 30;  // per-member edge columns up to 8 GB
 
 // Workspace layout for nmem members / njobs jobs with the given totals.
 template <typename T>
 RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
-                         unsigned long long ranges, unsigned long long maxm) {
+                         unsigned long long ranges, unsigned long long maxm, int max_swaths = 0) {
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   RoundLayout L;
   L.edge_stride = (maxm + 32 + 31) / 32 * 32;
   const size_t slots = size_t(round_grid<T>()) * kRoundWarps;
+  L.max_swaths = max_swaths;
+  L.pipe = max_swaths > 0 && size_t(nmem) * 2 * L.edge_stride * sizeof(T) <= kPipeEdgeBytes;
+  const size_t edge_cols = L.pipe ? size_t(nmem) : slots;
   size_t o = 0;
   L.off_counter = o; o += 256;
   L.off_path = o; o += up(size_t(nmem) * 8);
@@ -453,8 +584,11 @@ RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
   // single-job descriptors: mseries, mjob (nmem ints each), clen, jflags, mbeg, mend, coff
   L.off_single = o; o += up(size_t(nmem) * 8 + 64);
   L.off_ranges = o; o += up(size_t(ranges) * sizeof(int2));
-  L.off_edges = o; o += up(slots * 2 * L.edge_stride * sizeof(T));
+  L.off_edges = o; o += up(edge_cols * 2 * L.edge_stride * sizeof(T));
   L.off_words = o; o += up(words * 8);
+  const size_t ps = L.pipe ? size_t(nmem) * size_t(max_swaths) : 0;
+  L.off_prog = o; o += up(ps * 8);
+  L.off_emtop = o; o += up(ps * 2 * sizeof(T));
   L.total = o;
   (void)njobs;
   return L;
@@ -463,9 +597,10 @@ RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
 template <typename T>
 void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint64_t *h_clen,
                  const int *h_flags, unsigned long long &words, unsigned long long &ranges,
-                 unsigned long long &maxm) {
+                 unsigned long long &maxm, int *max_swaths = nullptr) {
   words = ranges = 0;
   maxm = 1;
+  if (max_swaths) *max_swaths = 1;
   for (int k = 0; k < nmem; ++k) {
     const int j = h_mjob ? h_mjob[k] : 0;
     const int f = h_flags[j];
@@ -474,6 +609,7 @@ void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint
     words += g.words;
     ranges += h_clen[j];
     if ((unsigned long long)g.m > maxm) maxm = g.m;
+    if (max_swaths && g.swaths > *max_swaths) *max_swaths = g.swaths;
   }
 }
 
@@ -489,14 +625,23 @@ int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen
   a.edges = reinterpret_cast<T *>(base + L.off_edges);
   a.edge_stride = L.edge_stride;
   a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
+  a.prog = reinterpret_cast<unsigned long long *>(base + L.off_prog);
+  a.emtop = reinterpret_cast<T *>(base + L.off_emtop);
+  a.err = reinterpret_cast<unsigned *>(base + L.off_counter + 8);
+  a.max_swaths = L.max_swaths;
   const unsigned long long nr = (L.off_edges - L.off_ranges) / sizeof(int2);
-  cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
+  cudaMemsetAsync(a.counter, 0, 16, stream);  // work counter and error word
   plan_kernel<T><<<1, 32, 0, stream>>>(a);
   fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
   // with fewer members than resident warps, one block per member spreads
   // them over the SMs instead of leaving them to the first blocks placed
   const bool spread = a.nmem < round_grid<T>() * kRoundWarps;
-  if (spread)
+  if (L.pipe) {
+    cudaMemsetAsync(a.prog, 0, size_t(a.nmem) * L.max_swaths * 8, stream);
+    path_pipe_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>
+        <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
+    shortcut_kernel<T><<<(a.nmem + 127) / 128, 128, 0, stream>>>(a);
+  } else if (spread)
     path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, 1><<<a.nmem, 32, 0, stream>>>(a);
   else
     path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, kRoundWarps>
@@ -514,9 +659,10 @@ size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int
   unsigned long long words, ranges, maxm;
   const uint64_t clen = Lc;
   const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm);
+  int ms = 1;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
   if (Lc > maxm) maxm = Lc;
-  return round_layout<T>(n, 1, words, ranges, maxm).total;
+  return round_layout<T>(n, 1, words, ranges, maxm, ms).total;
 }
 
 template <typename T>
@@ -527,9 +673,10 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
   unsigned long long words, ranges, maxm;
   const uint64_t clen = Lc;
   const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm);
+  int ms = 1;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
   if (Lc > maxm) maxm = Lc;
-  const RoundLayout L = round_layout<T>(n, 1, words, ranges, maxm);
+  const RoundLayout L = round_layout<T>(n, 1, words, ranges, maxm, ms);
   if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA round workspace too small");
   char *base = static_cast<char *>(ws);
   int *single = reinterpret_cast<int *>(base + L.off_single);
@@ -566,10 +713,11 @@ template <typename T>
 size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int nmem,
                                  const uint64_t *h_clen, const int *h_flags, int njobs) {
   unsigned long long words, ranges, maxm;
-  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm);
+  int ms = 1;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms);
   for (int j = 0; j < njobs; ++j)
     if (h_clen[j] > maxm) maxm = h_clen[j];
-  return round_layout<T>(nmem, njobs, words, ranges, maxm).total;
+  return round_layout<T>(nmem, njobs, words, ranges, maxm, ms).total;
 }
 
 template <typename T>
@@ -582,10 +730,11 @@ int dba_batch_launch(const T *centroids, const unsigned long long *coff, const i
                      int32_t *triples, int64_t *triple_counts, void *ws, size_t ws_bytes,
                      cudaStream_t stream) {
   unsigned long long words, ranges, maxm;
-  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm);
+  int ms = 1;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms);
   for (int j = 0; j < njobs; ++j)
     if (h_clen[j] > maxm) maxm = h_clen[j];
-  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm);
+  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm, ms);
   if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA batch workspace too small");
   RoundArgs<T> a;
   a.centroids = centroids;

@@ -84,10 +84,11 @@ struct TileIn {
 // Sweeps one swath recording moves.  Same wavefront as sweep_swath; in
 // addition lane 31 keeps the minimum of the right-edge column it spills and
 // its top-row value (for the reference's open-end shortcut, dtw.hpp:74-129).
-template <typename T, int R>
+template <typename T, int R, typename Gate = NoGate>
 __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const PathOut &po,
                                                  T (&col)[R], T &edge_min, T &edge_top,
-                                                 TileIn<T> tile = TileIn<T>{nullptr, -1}) {
+                                                 TileIn<T> tile = TileIn<T>{nullptr, -1},
+                                                 Gate gate = Gate()) {
   const int lane = threadIdx.x & 31;
   const int m = job.m;
   const int r0 = job.r0;
@@ -129,6 +130,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     xa = job.x[ia];
     xb = job.x[ib];
     if (has_in) {
+      if (Gate::kActive) gate.wait_in(rows > 0 ? kb + 1 : 0);
       ea = job.edge_in[ka];
       eb = job.edge_in[kb];
     } else {
@@ -197,6 +199,13 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     }
     cp_async_commit();
   };
+  // edge rows of chunk c must be published before any lane copies them
+  auto gate_chunk = [&](int c) {
+    if (Gate::kActive && has_in && lane0) {
+      const int need = (c + 1) * kChunkRows;
+      gate.wait_in(rows < need ? rows : need);
+    }
+  };
   auto staged = [&](int u, T &xa, T &xb, T &ea, T &eb) {
     using V2 = typename Pair2<T>::V;
     const T *slot = job.stage + ((u >> 5) & 1) * (2 * kChunkRows);
@@ -221,6 +230,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
   if (t < steady_end) {
     using V2 = typename Pair2<T>::V;
     const int cfirst = t >> 5;
+    gate_chunk(cfirst + 1);
     __syncwarp();
     issue_chunk(cfirst);
     issue_chunk(cfirst + 1);
@@ -234,9 +244,11 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
       T la = __shfl_up_sync(kFull, a_last, 1);
       T lb = __shfl_up_sync(kFull, col[R - 1], 1);
       if (((t + 1) & 31) == 0) {
+        const int c1 = (t + 1) >> 5;
         cp_async_wait_all();
+        gate_chunk(c1 + 1);
         __syncwarp();
-        issue_chunk(((t + 1) >> 5) + 1);
+        issue_chunk(c1 + 1);
       }
       if (lane0) {
         xa = pxa;
@@ -262,6 +274,8 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
           v.x = a_last;
           v.y = col[R - 1];
           *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
+          if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1)
+            gate.publish(2 * (t - 31) + 2);
         }
         emin = Num<T>::min2(emin, Num<T>::min2(a_last, col[R - 1]));
       }
@@ -271,6 +285,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     __syncwarp();
   }
   for (; t < total; ++t) masked_step(t);
+  if (Gate::kActive && lane31 && has_out) gate.publish(rows);
   edge_min = __shfl_sync(kFull, emin, 31);
   edge_top = __shfl_sync(kFull, etop, 31);
 }
