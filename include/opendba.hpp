@@ -89,12 +89,22 @@ void normalizeSequences(T **sequences, size_t num_sequences, size_t *sequence_le
                         int refSequenceIndex, double *sequence_means, double *sequence_sigmas,
                         cudaStream_t stream);
 
+// chopPrefixFromSequences<T> (dba.hpp:1193): aligns every series to the
+// leader with open-end DTW, writes <output_prefix>.prefix_chop.txt and replaces
+// each series by its tail from the chop position (empty ones are dropped).
+template <typename T>
+void chopPrefixFromSequences(T *sequence_prefix, size_t sequence_prefix_length, T **sequences,
+                             int *num_sequences, size_t *sequence_lengths, char **sequence_names,
+                             char *output_prefix, int norm_sequences, cudaStream_t stream = 0);
+
 template <typename T>
 void adaptive_segmentation(T **sequences, size_t *seq_lengths, int num_seqs, int min_segment_length,
                            T ***segmented_sequences, size_t **segmented_seq_lengths,
                            int prefix_length_to_skip, cudaStream_t stream = 0);
 
 #define ODBA_EXTERN_TEMPLATES(T)                                                               \
+  extern template void chopPrefixFromSequences<T>(T *, size_t, T **, int *, size_t *, char **,   \
+                                                  char *, int, cudaStream_t);                    \
   extern template void setupAndRun<T>(char *, char **, int, char *, int, int, int, char *, int, \
                                       double, const int, const int, bool);                     \
   extern template void performDBA<T>(T **, int, size_t *, char **, int, int, char *, int,       \

@@ -265,6 +265,27 @@ int odba_dba_round_stripe_f64(const double *centroid, uint64_t centroid_len, con
                               int32_t *path_triples, int64_t *path_counts, void *workspace,
                               size_t workspace_bytes, void *stream);
 
+/* ---- prefix chop -----------------------------------------------------------------
+ * Replaces the alignment and path walk of chopPrefixFromSequences<T>
+ * (dba.hpp:1191-1395): every series is aligned to the leader (prefix,
+ * P samples, on the rows) with open-end DTW and a recorded path; walking the
+ * path back from the end cell past the run of OPEN_RIGHT moves along the top
+ * row gives the chop position (chop_positions[k], the first column kept;
+ * -1 if the walk failed), and histograms[k * P + i] counts the path cells
+ * from there to (0, 0) on leader row i.  Device buffers; h_lens is a host copy
+ * of lens.  The caller normalises the leader and the series first (as the
+ * reference does when it normalises) and cuts the series. */
+size_t odba_prefix_chop_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
+                                        uint64_t prefix_len);
+int odba_prefix_chop_f32(const float *prefix, uint64_t prefix_len, const float *series,
+                         const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                         int64_t *chop_positions, int32_t *histograms, void *workspace,
+                         size_t workspace_bytes, void *stream);
+int odba_prefix_chop_f64(const double *prefix, uint64_t prefix_len, const double *series,
+                         const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                         int64_t *chop_positions, int32_t *histograms, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
 /* ---- one DBA round for many jobs at once ---------------------------------------
  * No single reference counterpart: DBAUpdate<T> (dba.hpp:432-848) for many
  * independent averaging jobs in one launch sequence (no host synchronization

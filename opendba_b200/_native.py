@@ -39,6 +39,9 @@ SIGNATURES = {
     "odba_cutree_cdist": (I32, [I32, P, P, ctypes.c_double, P]),
     "odba_cluster_medoids_f32": (I32, [I32, P, P, ctypes.c_double, P, P, P]),
     "odba_cluster_medoids_f64": (I32, [I32, P, P, ctypes.c_double, P, P, P]),
+    "odba_prefix_chop_workspace_bytes": (ctypes.c_size_t, [I32, P, I32, U64]),
+    "odba_prefix_chop_f32": (I32, [P, U64, P, P, P, P, I32, P, P, P, ctypes.c_size_t, P]),
+    "odba_prefix_chop_f64": (I32, [P, U64, P, P, P, P, I32, P, P, P, ctypes.c_size_t, P]),
     "odba_tune_set": (I32, [I32, I32, I32, I32]),
     "odba_tune_query": (I32, [I32, U64, U64, ctypes.c_size_t, P, P]),
     "odba_tune_mode": (None, [I32]),

@@ -182,6 +182,22 @@ int dba_round_checked(const T *centroid, uint64_t Lc, const T *series,
                              ws_bytes, static_cast<cudaStream_t>(stream));
 }
 
+template <typename T>
+int prefix_chop_checked(const T *prefix, uint64_t P, const T *series, const uint64_t *offsets,
+                               const uint64_t *lens, const uint64_t *h_lens, int n, int64_t *chop,
+                               int32_t *hist, void *ws, size_t ws_bytes, void *stream) {
+  if (n < 1 || P == 0 || !prefix || !series || !offsets || !lens || !h_lens || !chop || !hist || !ws)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer, empty prefix or no series");
+  if (P > (1ull << 30)) return fail(ODBA_ERR_INVALID_ARGUMENT, "prefix too long");
+  for (int k = 0; k < n; ++k)
+    if (h_lens[k] == 0 || h_lens[k] > (1ull << 30))
+      return fail(ODBA_ERR_INVALID_ARGUMENT, "series lengths must be in [1, 2^30]");
+  if (int rc = require_sm100()) return rc;
+  return prefix_chop_launch<T>(prefix, P, series, offsets, lens, h_lens, n,
+                               reinterpret_cast<long long *>(chop), hist, ws, ws_bytes,
+                               static_cast<cudaStream_t>(stream));
+}
+
 }  // namespace
 }  // namespace odba
 
@@ -409,6 +425,29 @@ int odba_dba_round_stripe_f64(const double *centroid, uint64_t centroid_len, con
                                    use_open_start, use_open_end, new_centroid, counts, delta,
                                    path_triples, path_counts, workspace, workspace_bytes, stream,
                                    ckpt_rows);
+}
+
+size_t odba_prefix_chop_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
+                                        uint64_t prefix_len) {
+  if (n < 1 || !h_lens || prefix_len == 0) return 0;
+  if (elem_size == 8) return prefix_chop_workspace_bytes<double>(h_lens, n, prefix_len);
+  return prefix_chop_workspace_bytes<float>(h_lens, n, prefix_len);
+}
+
+int odba_prefix_chop_f32(const float *prefix, uint64_t prefix_len, const float *series,
+                         const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                         int64_t *chop_positions, int32_t *histograms, void *workspace,
+                         size_t workspace_bytes, void *stream) {
+  return prefix_chop_checked<float>(prefix, prefix_len, series, offsets, lens, h_lens, n,
+                                    chop_positions, histograms, workspace, workspace_bytes, stream);
+}
+
+int odba_prefix_chop_f64(const double *prefix, uint64_t prefix_len, const double *series,
+                         const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens, int n,
+                         int64_t *chop_positions, int32_t *histograms, void *workspace,
+                         size_t workspace_bytes, void *stream) {
+  return prefix_chop_checked<double>(prefix, prefix_len, series, offsets, lens, h_lens, n,
+                                     chop_positions, histograms, workspace, workspace_bytes, stream);
 }
 
 size_t odba_dba_batch_workspace_bytes(int elem_size, const uint64_t *h_member_lens,

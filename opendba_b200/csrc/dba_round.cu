@@ -55,9 +55,10 @@ struct MemberGeom {
 };
 
 template <typename T>
-__host__ __device__ inline MemberGeom member_geom(uint64_t len, uint64_t Lc, int os, int oe) {
+__host__ __device__ inline MemberGeom member_geom(uint64_t len, uint64_t Lc, int os, int oe,
+                                                  int centroid_rows = 0) {
   MemberGeom g;
-  g.flip = (oe && Lc < len) ? 1 : 0;
+  g.flip = ((oe && Lc < len) || centroid_rows) ? 1 : 0;
   g.m = int(g.flip ? Lc : len);
   g.n = int(g.flip ? len : Lc);
   g.r0 = os ? 1 : 0;
@@ -69,7 +70,8 @@ __host__ __device__ inline MemberGeom member_geom(uint64_t len, uint64_t Lc, int
 }
 
 // Jobs share one launch: job J owns centroid centroids[coff[J] .. + clen[J]),
-// flags (bit 0 open start, bit 1 open end, bit 2 active) and the members
+// flags (bit 0 open start, bit 1 open end, bit 2 active, bit 3 centroid on
+// the rows whatever the lengths -- the prefix-chop orientation) and the members
 // job_mbeg[J] .. job_mend[J]-1 of the member list (member k is series
 // mem_series[k] of the series table).  Members of a job are contiguous and in
 // the job's order, which is the order their samples are added.
@@ -112,7 +114,8 @@ template <typename T>
 __device__ __forceinline__ MemberGeom geom_of(const RoundArgs<T> &a, int k, int &job) {
   job = a.mjob[k];
   const int f = a.jflags[job];
-  return member_geom<T>(a.lens[a.mseries[k]], uint64_t(a.clen[job]), f & 1, (f >> 1) & 1);
+  return member_geom<T>(a.lens[a.mseries[k]], uint64_t(a.clen[job]), f & 1, (f >> 1) & 1,
+                        (f >> 3) & 1);
 }
 
 // Members of inactive jobs take no path words and no ranges (a caller can run
@@ -261,7 +264,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_pipe_kernel(RoundArgs<T
     const MemberGeom g = geom_of<T>(a, k, jb);
     const int flags = a.jflags[jb];
     if (!(flags & 4) || s >= g.swaths) continue;
-    const int os = flags & 1, oe = (flags >> 1) & 1;
+    const int oe = (flags >> 1) & 1;
     const T *seq = a.series + a.offsets[a.mseries[k]];
     const T *cen = a.centroids + a.coff[jb];
     T *b0 = a.edges + (unsigned long long)k * 2 * a.edge_stride;
@@ -348,64 +351,33 @@ __global__ void shortcut_kernel(RoundArgs<T> a) {
   a.shortcut[k] = shortcut;
 }
 
-// The backtrack (updateCentroid's loop, dba.hpp:374-423): one warp per
-// member walks its path from the end cell back to (0, 0).  Every lane holds
-// the move word of one of the 32 rows at and below the current cell (the
-// word of the lane that owned the current column in the path sweep), so the
-// walk advances by shuffles and reloads only when it leaves those 32 rows or
-// that owner's columns -- about once per 32 steps instead of one dependent
-// global load per step.  Every lane keeps the same walk state; lane 0 stores
-// the per-centroid-index sample ranges and, if asked, the path listing.
-// Moves are decoded as the reference defines them: the open-end shortcut
-// overrides the top row first (with a single-row matrix that row is row 0,
-// dtw.hpp:105-108 runs before the row-0 loop), then row 0 (RIGHT or
-// OPEN_RIGHT, NIL / NIL_OPEN_RIGHT at (0, 0)), then the recorded code with
-// RIGHT on the open-end top row meaning OPEN_RIGHT.
-template <typename T>
-__global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T> a) {
+// Walks member k's path from its end cell toward (0, 0) with one warp and
+// calls visit(move, r, c) for every cell; the last call has NIL or
+// NIL_OPEN_RIGHT.  Returns false if the walk failed.  Every lane holds the
+// move word of one of the 32 rows at and below the current cell (the word of
+// the lane that owned the current column in the path sweep), so the walk
+// advances by shuffles and reloads only when it leaves those 32 rows or that
+// owner's columns -- about once per 32 steps instead of one dependent global
+// load per step.  Every lane keeps the same walk state (visitors store from
+// lane 0 only).  Moves are decoded as the reference defines them: the
+// open-end shortcut overrides the top row first (with a single-row matrix that
+// row is row 0, dtw.hpp:105-108 runs before the row-0 loop), then row 0
+// (RIGHT or OPEN_RIGHT, NIL / NIL_OPEN_RIGHT at (0, 0)), then the recorded
+// code with RIGHT on the open-end top row meaning OPEN_RIGHT.
+template <typename T, typename Visit>
+__device__ __forceinline__ bool walk_member_path(const RoundArgs<T> &a, const MemberGeom &g, int k,
+                                                 int os, int oe, Visit &&visit) {
   const int lane = threadIdx.x & 31;
-  const int k = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
-  if (k >= a.nmem) return;
-  int jb;
-  const MemberGeom g = geom_of<T>(a, k, jb);
-  const int flags = a.jflags[jb];
-  if (!(flags & 4)) return;
-  const int os = flags & 1, oe = (flags >> 1) & 1;
   constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
-  int2 *rg = a.ranges + a.rng_off[k];
-  int32_t *tri = a.triples ? a.triples + 3ull * a.trip_off[k] : nullptr;
-  const bool lead = lane == 0;
-  long long nt = 0;
-  int r = g.m - 1, c = g.n - 1;
-  int cur_t = -1, lo = 1, hi = 0;
-  auto contribute = [&](int rr, int cc) {
-    const int ti = g.flip ? rr : cc;  // centroid index
-    const int mi = g.flip ? cc : rr;  // member sample index
-    if (ti != cur_t) {
-      if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
-      cur_t = ti;
-      lo = mi;
-      hi = mi;
-    } else {
-      lo = mi;  // the walk only moves toward smaller indices
-    }
-  };
-  auto emit = [&](int mv) {
-    if (lead && tri) {
-      tri[3 * nt] = r;
-      tri[3 * nt + 1] = c;
-      tri[3 * nt + 2] = mv;
-    }
-    ++nt;
-  };
   // A path has at most m + n - 1 cells and never leaves the matrix; the checks
   // only keep a corrupt path buffer from turning into an endless or
-  // out-of-bounds walk (the member is then reported with a count of -1).
+  // out-of-bounds walk.
   const long long max_cells = (long long)g.m + g.n - 1;
-  bool failed = false, done = false;
-  while (!done && !failed) {
+  long long steps = 0;
+  int r = g.m - 1, c = g.n - 1;
+  for (;;) {
     const int s = c / W, c0 = s * W;
     int R = RF;
     if (s == g.swaths - 1) {
@@ -432,19 +404,12 @@ __global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T
         if (mv == kMoveRight && oe && r == g.m - 1) mv = kMoveOpenRight;
       }
       if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {
-        // the start cell (dba.hpp:412-415)
-        if (mv != kMoveNilOpenRight) contribute(0, 0);
-        if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
-        emit(mv);
-        done = true;
-        break;
+        visit(mv, r, c);
+        return true;
       }
-      if (nt >= max_cells - 1) {
-        failed = true;
-        break;
-      }
-      emit(mv);
-      if (mv != kMoveOpenRight) contribute(r, c);
+      if (steps >= max_cells - 1) return false;
+      visit(mv, r, c);
+      ++steps;
       if (mv == kMoveDiag) {
         --r;
         --c;
@@ -453,14 +418,102 @@ __global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T
       } else {
         --c;
       }
-      if (r < 0 || c < 0) {
-        failed = true;
-        break;
-      }
+      if (r < 0 || c < 0) return false;
       if (top - r >= 32 || c < cbeg) break;  // reload the window
     }
   }
-  if (lead && a.triple_counts) a.triple_counts[k] = failed ? -1 : nt;
+}
+
+// The backtrack (updateCentroid's loop, dba.hpp:374-423): per member the
+// contiguous range of member samples each centroid index receives, and the
+// path listing if asked.  One warp per member.
+template <typename T>
+__global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T> a) {
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
+  if (k >= a.nmem) return;
+  int jb;
+  const MemberGeom g = geom_of<T>(a, k, jb);
+  const int flags = a.jflags[jb];
+  if (!(flags & 4)) return;
+  const int os = flags & 1, oe = (flags >> 1) & 1;
+  int2 *rg = a.ranges + a.rng_off[k];
+  int32_t *tri = a.triples ? a.triples + 3ull * a.trip_off[k] : nullptr;
+  const bool lead = lane == 0;
+  long long nt = 0;
+  int cur_t = -1, lo = 1, hi = 0;
+  auto contribute = [&](int rr, int cc) {
+    const int ti = g.flip ? rr : cc;  // centroid index
+    const int mi = g.flip ? cc : rr;  // member sample index
+    if (ti != cur_t) {
+      if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
+      cur_t = ti;
+      lo = mi;
+      hi = mi;
+    } else {
+      lo = mi;  // the walk only moves toward smaller indices
+    }
+  };
+  const bool ok = walk_member_path<T>(a, g, k, os, oe, [&](int mv, int r, int c) {
+    if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {
+      // the start cell (dba.hpp:412-415)
+      if (mv != kMoveNilOpenRight) contribute(0, 0);
+      if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
+    } else if (mv != kMoveOpenRight) {
+      contribute(r, c);
+    }
+    if (lead && tri) {
+      tri[3 * nt] = r;
+      tri[3 * nt + 1] = c;
+      tri[3 * nt + 2] = mv;
+    }
+    ++nt;
+  });
+  if (lead && a.triple_counts) a.triple_counts[k] = ok ? nt : -1;
+}
+
+// Prefix chop (chopPrefixFromSequences' host walk, dba.hpp:1313-1336), on
+// each series' open-end path against the leader (leader on the rows): skip
+// the OPEN_RIGHT run along the top row from the end cell; the column reached
+// is the chop position; then count, per leader row, the path cells from there
+// to (0, 0) (the cell reached counts 1 on the top row).  One warp per series;
+// rows are visited in one run each, so each count is stored once.
+template <typename T>
+__global__ void __launch_bounds__(kRoundWarps * 32) chop_walk_kernel(RoundArgs<T> a, long long *chop,
+                                                                    int *hist, int P) {
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
+  if (k >= a.nmem) return;
+  int jb;
+  const MemberGeom g = geom_of<T>(a, k, jb);
+  const int flags = a.jflags[jb];
+  if (!(flags & 4)) return;
+  const bool lead = lane == 0;
+  int *h = hist + (unsigned long long)k * P;
+  bool skipping = true;
+  long long pos = -1;
+  int row = -1, count = 0;
+  const bool ok = walk_member_path<T>(a, g, k, flags & 1, (flags >> 1) & 1, [&](int mv, int r, int c) {
+    if (skipping) {
+      if (mv == kMoveOpenRight) return;
+      skipping = false;
+      pos = c;
+      row = r;
+      count = 1;
+      return;
+    }
+    if (r == row) {
+      ++count;
+    } else {
+      if (lead) h[row] = count;
+      row = r;
+      count = 1;
+    }
+  });
+  if (lead) {
+    if (ok && row >= 0) h[row] = count;
+    chop[k] = ok ? pos : -1;
+  }
 }
 
 // The reference divides on the host (dba.hpp:820-822); a centroid index that
@@ -605,7 +658,7 @@ void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint
     const int j = h_mjob ? h_mjob[k] : 0;
     const int f = h_flags[j];
     if (!(f & 4)) continue;
-    const MemberGeom g = member_geom<T>(h_lens[k], h_clen[j], f & 1, (f >> 1) & 1);
+    const MemberGeom g = member_geom<T>(h_lens[k], h_clen[j], f & 1, (f >> 1) & 1, (f >> 3) & 1);
     words += g.words;
     ranges += h_clen[j];
     if ((unsigned long long)g.m > maxm) maxm = g.m;
@@ -613,9 +666,10 @@ void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint
   }
 }
 
+// Planning, range clearing and the path DTW of a round (everything before
+// the backtrack).
 template <typename T>
-int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen,
-                 cudaStream_t stream) {
+void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_t stream) {
   a.counter = reinterpret_cast<unsigned long long *>(base + L.off_counter);
   a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
   a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
@@ -646,6 +700,12 @@ int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen
   else
     path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, kRoundWarps>
         <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
+}
+
+template <typename T>
+int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen,
+                 cudaStream_t stream) {
+  launch_paths<T>(a, L, base, stream);
   backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
   dim3 rg((max_clen + 255) / 256, a.njobs);
   reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
@@ -1242,6 +1302,83 @@ template int dba_round_stripe_launch<double>(const double *, uint64_t, const dou
                                              const uint64_t *, const uint64_t *, const uint64_t *,
                                              int, int, int, int, double *, uint32_t *, double *,
                                              int32_t *, int64_t *, void *, size_t, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Prefix chop (chopPrefixFromSequences, dba.hpp:1191-1395): every series is
+// aligned to the leader with open-end DTW and a recorded path (leader on the
+// rows, whatever the lengths), by the DBA round's path kernels; then one warp
+// per series walks its path (chop_walk_kernel).
+namespace {
+constexpr int kChopFlags = 2 | 4 | 8;  // open end, active, centroid (the leader) on the rows
+}  // namespace
+
+template <typename T>
+size_t prefix_chop_workspace_bytes(const uint64_t *h_lens, int n, uint64_t P) {
+  unsigned long long words, ranges, maxm;
+  const uint64_t clen = P;
+  const int flags = kChopFlags;
+  int ms = 1;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
+  if (P > maxm) maxm = P;
+  return round_layout<T>(n, 1, words, ranges, maxm, ms).total;
+}
+
+template <typename T>
+int prefix_chop_launch(const T *prefix, uint64_t P, const T *series, const uint64_t *offsets,
+                       const uint64_t *lens, const uint64_t *h_lens, int n, long long *chop,
+                       int *hist, void *ws, size_t ws_bytes, cudaStream_t stream) {
+  unsigned long long words, ranges, maxm;
+  const uint64_t clen = P;
+  const int flags = kChopFlags;
+  int ms = 1;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
+  if (P > maxm) maxm = P;
+  const RoundLayout L = round_layout<T>(n, 1, words, ranges, maxm, ms);
+  if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "prefix chop workspace too small");
+  char *base = static_cast<char *>(ws);
+  int *single = reinterpret_cast<int *>(base + L.off_single);
+  int *mseries = single, *mjob = single + n, *d_clen = single + 2 * n, *d_flags = single + 2 * n + 1,
+      *d_mbeg = single + 2 * n + 2, *d_mend = single + 2 * n + 3;
+  unsigned long long *d_coff =
+      reinterpret_cast<unsigned long long *>(base + L.off_single + ((size_t(2 * n + 4) * 4 + 7) / 8) * 8);
+  single_job_kernel<<<(n + 255) / 256, 256, 0, stream>>>(mseries, mjob, n, d_clen, int(P), d_flags,
+                                                        flags, d_mbeg, d_mend, d_coff);
+  RoundArgs<T> a;
+  a.centroids = prefix;
+  a.coff = d_coff;
+  a.clen = d_clen;
+  a.jflags = d_flags;
+  a.mbeg = d_mbeg;
+  a.mend = d_mend;
+  a.njobs = 1;
+  a.series = series;
+  a.offsets = offsets;
+  a.lens = lens;
+  a.mseries = mseries;
+  a.mjob = mjob;
+  a.order = nullptr;
+  a.nmem = n;
+  a.means = nullptr;
+  a.counts = nullptr;
+  // the planner clears the job's delta: a spare word of the counter block
+  a.deltas = reinterpret_cast<double *>(base + L.off_counter + 16);
+  a.triples = nullptr;
+  a.triple_counts = nullptr;
+  cudaMemsetAsync(hist, 0, size_t(n) * P * sizeof(int), stream);
+  launch_paths<T>(a, L, base, stream);
+  chop_walk_kernel<T><<<(n + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a, chop, hist,
+                                                                                          int(P));
+  return check_launch("prefix chop kernels");
+}
+
+template size_t prefix_chop_workspace_bytes<float>(const uint64_t *, int, uint64_t);
+template size_t prefix_chop_workspace_bytes<double>(const uint64_t *, int, uint64_t);
+template int prefix_chop_launch<float>(const float *, uint64_t, const float *, const uint64_t *,
+                                       const uint64_t *, const uint64_t *, int, long long *, int *,
+                                       void *, size_t, cudaStream_t);
+template int prefix_chop_launch<double>(const double *, uint64_t, const double *, const uint64_t *,
+                                        const uint64_t *, const uint64_t *, int, long long *, int *,
+                                        void *, size_t, cudaStream_t);
 
 template size_t dba_round_workspace_bytes<float>(const uint64_t *, int, uint64_t, int, int);
 template size_t dba_round_workspace_bytes<double>(const uint64_t *, int, uint64_t, int, int);

@@ -941,6 +941,69 @@ int write_sequences(T **seqs, size_t *lens, char **names, int n, const std::stri
   return 0;
 }
 
+// The alignment half of chopPrefixFromSequences (dba.hpp:1191-1336): with
+// norm, the leader and the series are z-normalised (the series in place, as
+// the reference does to its managed copies); then every series' chop position
+// and leader-row histogram.
+template <typename T>
+void prefix_chop_core(const T *prefix, size_t P, T **seqs, const size_t *lens, int n, int norm,
+                      std::vector<long long> &chop, std::vector<int> &hist, cudaStream_t st) {
+  DeviceSet<T> ds;
+  ds.upload(seqs, lens, n, st);
+  DevBuf d_pre((P + 16) * sizeof(T));
+  check_cuda(cudaMemcpyAsync(d_pre.p, prefix, P * sizeof(T), cudaMemcpyDefault, st), "prefix upload");
+  if (norm) {
+    const uint64_t zero = 0, plen = P;
+    DevBuf po(sizeof(uint64_t)), pl(sizeof(uint64_t));
+    check_cuda(cudaMemcpyAsync(po.p, &zero, 8, cudaMemcpyHostToDevice, st), "prefix offset");
+    check_cuda(cudaMemcpyAsync(pl.p, &plen, 8, cudaMemcpyHostToDevice, st), "prefix length");
+    check(Ops<T>::znorm(ptr<T>(d_pre), ptr<uint64_t>(po), ptr<uint64_t>(pl), 1, nullptr, nullptr, st),
+          "prefix z-normalisation");
+    check(Ops<T>::znorm(ptr<T>(ds.data), ptr<uint64_t>(ds.offs), ptr<uint64_t>(ds.lens), n, nullptr,
+                        nullptr, st),
+          "z-normalisation for prefix chopping");
+    for (int i = 0; i < n; ++i)
+      check_cuda(cudaMemcpyAsync(seqs[i], ptr<T>(ds.data) + ds.h_offs[i], lens[i] * sizeof(T),
+                                 cudaMemcpyDefault, st),
+                 "normalised series write-back");
+    check_cuda(cudaStreamSynchronize(st), "z-normalisation for prefix chopping");
+  }
+  DevBuf ws(odba_prefix_chop_workspace_bytes(sizeof(T), ds.h_lens.data(), n, P));
+  DevBuf d_chop(n * sizeof(long long)), d_hist(size_t(n) * P * sizeof(int));
+  check(sizeof(T) == 4
+            ? odba_prefix_chop_f32(reinterpret_cast<const float *>(d_pre.p), P,
+                                   reinterpret_cast<const float *>(ds.data.p), ptr<uint64_t>(ds.offs),
+                                   ptr<uint64_t>(ds.lens), ds.h_lens.data(), n,
+                                   reinterpret_cast<int64_t *>(d_chop.p), ptr<int32_t>(d_hist), ws.p,
+                                   ws.bytes, st)
+            : odba_prefix_chop_f64(reinterpret_cast<const double *>(d_pre.p), P,
+                                   reinterpret_cast<const double *>(ds.data.p), ptr<uint64_t>(ds.offs),
+                                   ptr<uint64_t>(ds.lens), ds.h_lens.data(), n,
+                                   reinterpret_cast<int64_t *>(d_chop.p), ptr<int32_t>(d_hist), ws.p,
+                                   ws.bytes, st),
+        "prefix chop");
+  chop.assign(n, 0);
+  hist.assign(size_t(n) * P, 0);
+  check_cuda(cudaMemcpyAsync(chop.data(), d_chop.p, n * sizeof(long long), cudaMemcpyDeviceToHost, st),
+             "chop positions");
+  check_cuda(cudaMemcpyAsync(hist.data(), d_hist.p, size_t(n) * P * sizeof(int), cudaMemcpyDeviceToHost, st),
+             "leader histograms");
+  check_cuda(cudaStreamSynchronize(st), "prefix chop");
+  for (int i = 0; i < n; ++i)
+    if (chop[i] < 0) {
+      std::cerr << "Prefix chop: the path walk of series " << i << " failed" << std::endl;
+      die(odba_exit::DEVICE_LIBRARY_ERROR);
+    }
+}
+
+// One line of <prefix>.prefix_chop.txt (dba.hpp:1346-1351).
+void write_chop_line(std::ofstream &f, const char *name, long long chop, size_t len, const int *hist,
+                     size_t P) {
+  f << name << "\t" << chop << "\t" << len;
+  for (size_t j = 0; j < P; ++j) f << "\t" << hist[j];
+  f << std::endl;
+}
+
 }  // namespace
 
 template <typename T>
@@ -993,9 +1056,43 @@ void setupAndRun(char *seqprefix_file_name, char **series_file_names, int num_se
     const size_t dot = nm.find('.');
     if (dot != std::string::npos) nm.resize(dot);
   }
+  // Step 1: chop a leading sequence off all inputs (openDBA.cuh:61-83, dba.hpp:1191-1395)
   if (seqprefix_file_name != nullptr) {
-    std::cerr << "Prefix chopping (a leader sequence) is not available in this build" << std::endl;
-    die(odba_exit::CANNOT_READ_SEQUENCE_PREFIX_FILE);
+    std::vector<T> leader;
+    const bool binary = read_mode == BINARY_READ_MODE;
+    const int rc = binary ? read_binary_data<T>(seqprefix_file_name, leader, false)
+                          : read_text_data<T>(seqprefix_file_name, leader);
+    if (rc || leader.empty()) {
+      std::cerr << "Cannot read prefix " << (binary ? "binary" : "text") << " data from "
+                << seqprefix_file_name << ", aborting" << std::endl;
+      die(odba_exit::CANNOT_READ_SEQUENCE_PREFIX_FILE);
+    }
+    std::vector<T *> ptrs(n);
+    std::vector<size_t> lns(n);
+    for (int i = 0; i < n; ++i) {
+      ptrs[i] = data[i].data();
+      lns[i] = data[i].size();
+    }
+    std::vector<long long> chop;
+    std::vector<int> hist;
+    prefix_chop_core<T>(leader.data(), leader.size(), ptrs.data(), lns.data(), n, norm_sequences,
+                        chop, hist, 0);
+    std::ofstream cf((std::string(output_prefix) + ".prefix_chop.txt").c_str());
+    std::vector<std::vector<T>> kept;
+    std::vector<std::string> kept_names;
+    for (int i = 0; i < n; ++i) {
+      write_chop_line(cf, names[i].c_str(), chop[i], lns[i], hist.data() + size_t(i) * leader.size(),
+                      leader.size());
+      if (lns[i] - size_t(chop[i]) == 0) {
+        std::cerr << "Skipping " << names[i] << " due to zero-length after prefix chopping" << std::endl;
+        continue;
+      }
+      kept.emplace_back(data[i].begin() + chop[i], data[i].end());
+      kept_names.push_back(names[i]);
+    }
+    data.swap(kept);
+    names.swap(kept_names);
+    n = int(data.size());
   }
   std::vector<T *> seq_ptrs(n);
   std::vector<size_t> lens(n);
@@ -1070,7 +1167,53 @@ void setupAndRun(char *seqprefix_file_name, char **series_file_names, int num_se
   for (auto p : name_ptrs) delete[] p;
 }
 
+// chopPrefixFromSequences<T> (dba.hpp:1191-1395) with the reference's
+// signature and side effects: with norm_sequences the caller's series are
+// z-normalised in place; <output_prefix>.prefix_chop.txt is written; every
+// series is replaced by a new cudaMallocManaged copy of its chopped tail (the
+// old array is released with cudaFree when it is CUDA memory, as the
+// reference's managed inputs are); series left empty are dropped and
+// *num_sequences shrinks.
+template <typename T>
+void chopPrefixFromSequences(T *sequence_prefix, size_t sequence_prefix_length, T **sequences,
+                             int *num_sequences, size_t *sequence_lengths, char **sequence_names,
+                             char *output_prefix, int norm_sequences, cudaStream_t stream) {
+  const int n = *num_sequences;
+  const size_t P = sequence_prefix_length;
+  std::vector<long long> chop;
+  std::vector<int> hist;
+  prefix_chop_core<T>(sequence_prefix, P, sequences, sequence_lengths, n, norm_sequences, chop, hist,
+                      stream);
+  std::ofstream cf((std::string(output_prefix) + ".prefix_chop.txt").c_str());
+  int out = 0;
+  for (int i = 0; i < n; ++i) {
+    write_chop_line(cf, sequence_names[i], chop[i], sequence_lengths[i], hist.data() + size_t(i) * P, P);
+    const size_t kept = sequence_lengths[i] - size_t(chop[i]);
+    cudaPointerAttributes attr;
+    const bool cuda_mem = cudaPointerGetAttributes(&attr, sequences[i]) == cudaSuccess &&
+                          (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    if (kept == 0) {
+      std::cerr << "Skipping " << sequence_names[i] << " due to zero-length after prefix chopping" << std::endl;
+      if (cuda_mem) cudaFree(sequences[i]);
+      continue;
+    }
+    T *ns = nullptr;
+    check_cuda(cudaMallocManaged(&ns, sizeof(T) * kept), "chopped sequence");
+    check_cuda(cudaMemcpy(ns, sequences[i] + chop[i], sizeof(T) * kept, cudaMemcpyDefault),
+               "chopped sequence copy");
+    if (cuda_mem) cudaFree(sequences[i]);
+    sequences[out] = ns;
+    sequence_lengths[out] = kept;
+    sequence_names[out] = sequence_names[i];
+    ++out;
+  }
+  *num_sequences = out;
+}
+
 #define ODBA_INSTANTIATE(T)                                                                     \
+  template void chopPrefixFromSequences<T>(T *, size_t, T **, int *, size_t *, char **, char *,  \
+                                           int, cudaStream_t);                                   \
   template void setupAndRun<T>(char *, char **, int, char *, int, int, int, char *, int, double, \
                                const int, const int, bool);                                     \
   template void performDBA<T>(T **, int, size_t *, char **, int, int, char *, int, double,       \

@@ -85,6 +85,13 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
                             size_t ws_bytes, cudaStream_t stream);
 
 template <typename T>
+size_t prefix_chop_workspace_bytes(const uint64_t *h_lens, int n, uint64_t P);
+template <typename T>
+int prefix_chop_launch(const T *prefix, uint64_t P, const T *series, const uint64_t *offsets,
+                       const uint64_t *lens, const uint64_t *h_lens, int n, long long *chop,
+                       int *hist, void *ws, size_t ws_bytes, cudaStream_t stream);
+
+template <typename T>
 size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int nmem,
                                  const uint64_t *h_clen, const int *h_flags, int njobs);
 template <typename T>

@@ -265,3 +265,29 @@ def _long_round(raw):
             "forward_cells": cells, "gcups": cells / ms / 1e6, "workspace_gb": nbytes / 1e9,
             "full_path_would_need_tb": full_path_tb, "delta": float(delta),
             "finite_mean": bool(torch.isfinite(mean).all().item())}
+
+
+def run_round(n_members=400, len_lo=3000, len_hi=8000, seed=synth.SEED_BASE + 6, reps=3):
+    """One full-path DBA round (float32, global): n_members z-normalised step
+    signals of U[len_lo, len_hi] samples against member 7 as the centroid;
+    CUDA-event time per round over ``reps`` rounds after two warm-up rounds."""
+    import torch
+    rng = np.random.default_rng(seed)
+    mem = synth.step_signals(rng, rng.integers(len_lo, len_hi + 1, n_members), 90, 12, 10, 2)
+    ds = api.DeviceSeries.from_host(mem)
+    api.znorm_(ds)
+    c = ds.data[int(ds.offsets[7]):int(ds.offsets[7]) + len(mem[7])].clone()
+    for _ in range(2):
+        api.dba_round(c, ds, 0, 0)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        api.dba_round(c, ds, 0, 0)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    cells = float(sum(len(m) for m in mem)) * len(c)
+    return {"workload": f"one DBA round, {n_members} members U[{len_lo},{len_hi}] vs a {len(c)}-sample "
+                        "centroid, global, float32", "round_ms": ms, "cells": cells,
+            "gcups": cells / ms / 1e6}

@@ -26,7 +26,8 @@
 //   performdba <in.odbs> <out_prefix> <open_start> <open_end> <norm> [cdist]
 //       performDBA (dba.hpp:863-1189), CLUSTER_AND_CONSENSUS, cdist default 1.
 //   setupandrun <out_prefix> <open_start> <open_end> <norm> <file>...
-//       setupAndRun<float> on text files, as tests/openDBA_test.cu does.
+//       setupAndRun<float> on text files, as tests/openDBA_test.cu does; with
+//       ODBA_HARNESS_SEQPREFIX=<leader text file> it chops that prefix first.
 //   segment    <in.odbs> <out.odbs> <min_segment_length> <prefix_skip>
 //       adaptive_segmentation (segmentation.hpp:340-583).
 #include <cfloat>
@@ -268,8 +269,13 @@ int main(int argc, char **argv) {
       std::memcpy(files[i], argv[6 + i], len);
     }
     char minseg[8] = "0";
-    setupAndRun<float>(nullptr, files, nfiles, pfx.data(), TEXT_READ_MODE, std::atoi(argv[3]),
-                       std::atoi(argv[4]), minseg, std::atoi(argv[5]), 1.0);
+    // a leader (prefix) file for the prefix chop, if given in the environment
+    std::vector<char> leader;
+    if (const char *lp = std::getenv("ODBA_HARNESS_SEQPREFIX"))
+      leader.assign(lp, lp + std::strlen(lp) + 1);
+    setupAndRun<float>(leader.empty() ? nullptr : leader.data(), files, nfiles, pfx.data(),
+                       TEXT_READ_MODE, std::atoi(argv[3]), std::atoi(argv[4]), minseg,
+                       std::atoi(argv[5]), 1.0);
   } else {
     SeriesBundle b = read_bundle(argv[2]);
     bool dbl = b.elem_size == 8;

@@ -7,7 +7,7 @@ committed copy lives in tests/golden/ref/; tests compare the CUDA path and
 the CPU oracle against it.
 
 Run on a B200 box from the repository root:
-    python tests/golden/make_reference_golden.py [out_dir] [--clusters-only]
+    python tests/golden/make_reference_golden.py [out_dir] [--clusters-only | --chop-only]
 """
 from __future__ import annotations
 
@@ -96,6 +96,49 @@ def family_series(dtype, seed, n_per=(9, 8, 7)):
     return [out[i] for i in order]
 
 
+def chop_inputs(dirname, seed):
+    """A leader (step signal, 300 samples) and reads that start with a warped,
+    noisy copy of it followed by a random tail; text files as setupAndRun reads."""
+    rng = np.random.default_rng(seed)
+    leader = synth.step_signal(rng, 300, 90.0, 12.0, 10.0, 2.0)
+    paths = []
+    os.makedirs(dirname, exist_ok=True)
+    for i in range(8):
+        L = int(rng.integers(220, 420))
+        t = np.sort(rng.random(L)) * (len(leader) - 1)
+        head = np.interp(t, np.arange(len(leader)), leader) + rng.normal(0, 1.5, L)
+        tail = synth.step_signal(rng, int(rng.integers(400, 1500)), 90.0, 12.0, 10.0, 2.0)
+        x = np.concatenate([head, tail])
+        p = os.path.join(dirname, f"read{i}.txt")
+        with open(p, "w") as f:
+            f.write("\n".join("%.4f" % v for v in x) + "\n")
+        paths.append(p)
+    lp = os.path.join(dirname, "leader.txt")
+    with open(lp, "w") as f:
+        f.write("\n".join("%.4f" % v for v in leader) + "\n")
+    return lp, paths
+
+
+def chop_cases(out, tmp, log):
+    """setupAndRun with a leader file: prefix_chop.txt, then DBA on the tails."""
+    d = os.path.join(out, "chop_inputs")
+    lp, paths = chop_inputs(d, synth.SEED_BASE + 606)
+    for norm in (1, 0):
+        pfx = os.path.join(tmp, f"chop_n{norm}")
+        env = dict(os.environ, ODBA_HARNESS_SEQPREFIX=lp)
+        t0 = time.time()
+        # file names relative to the input directory: the series names are the
+        # file names up to the first "." (openDBA.cuh:58-59)
+        p = subprocess.run([HARNESS, "setupandrun", pfx, "0", "0", str(norm)] +
+                           [os.path.basename(x) for x in paths],
+                           capture_output=True, text=True, env=env, cwd=d)
+        log.write(json.dumps({"args": ["setupandrun", pfx, 0, 0, norm], "rc": p.returncode,
+                              "secs": round(time.time() - t0, 3), "stderr": p.stderr[-2000:]}) + "\n")
+        for ext in (".prefix_chop.txt", ".avg.txt", ".pair_dists.txt"):
+            if os.path.exists(pfx + ext):
+                shutil.copy(pfx + ext, os.path.join(out, f"chop_n{norm}{ext}"))
+
+
 def cluster_cases(out, tmp, log):
     """performDBA with clustering thresholds other than 1 (dba.hpp:219-343,
     951-962): membership file, per-cluster averages and pair distances."""
@@ -119,6 +162,12 @@ def main():
     os.makedirs(out, exist_ok=True)
     tmp = os.path.join(out, "_tmp")
     os.makedirs(tmp, exist_ok=True)
+    if "--chop-only" in sys.argv:
+        with open(os.path.join(out, "harness_log_chop.jsonl"), "w") as log:
+            chop_cases(out, tmp, log)
+        shutil.rmtree(tmp, ignore_errors=True)
+        print("prefix chop golden written to", out)
+        return
     if "--clusters-only" in sys.argv:
         with open(os.path.join(out, "harness_log_clusters.jsonl"), "w") as log:
             cluster_cases(out, tmp, log)
@@ -225,12 +274,15 @@ def main():
     # 8. clustering thresholds other than 1
     with open(os.path.join(out, "harness_log_clusters.jsonl"), "w") as clog:
         cluster_cases(out, tmp, clog)
+    # 9. prefix chop with a leader sequence
+    with open(os.path.join(out, "harness_log_chop.jsonl"), "w") as clog:
+        chop_cases(out, tmp, clog)
 
     with open(os.path.join(out, "meta.json"), "w") as f:
         json.dump(meta, f, indent=1)
     shutil.rmtree(tmp, ignore_errors=True)
 
-    # 9. timing only (not a fixture): the reference's medoid launches on the first
+    # 10. timing only (not a fixture): the reference's medoid launches on the first
     # 40 rows of the 2000-series nanopore-like workload.
     if "--timing" in sys.argv:
         c2 = synth.znorm_host(synth.nanopore_like(2000, 2000, 8000, synth.SEED_BASE + 2))

@@ -182,3 +182,20 @@ def test_perform_dba_clusters_byte_identical(built, tmp_path, tag):
            f"cdist={float(c)})")
     for ext in (".cluster_membership.txt", ".avg.txt", ".pair_dists.txt"):
         assert _read(prefix + ext) == _read(gold + ext), ext
+
+
+@pytest.mark.parametrize("norm", [1, 0])
+def test_setup_and_run_prefix_chop_byte_identical(built, tmp_path, norm):
+    # setupAndRun with a leader file: the reference's prefix_chop.txt (chop
+    # positions, lengths, leader-row histograms) and the averages of the tails
+    d = os.path.join(GOLDEN, "chop_inputs")
+    gold = os.path.join(GOLDEN, f"chop_n{norm}")
+    if not os.path.exists(gold + ".prefix_chop.txt"):
+        pytest.skip("prefix chop golden files not generated")
+    files = sorted(f for f in os.listdir(d) if f.startswith("read"))
+    prefix = str(tmp_path / f"chop_n{norm}")
+    _child("from opendba_b200 import api\n"
+           f"api.setup_and_run({files!r}, {prefix!r}, 0, 0, 0, '0', {norm}, 1.0, "
+           f"seqprefix_file={os.path.join(d, 'leader.txt')!r})", cwd=d)
+    for ext in (".prefix_chop.txt", ".avg.txt", ".pair_dists.txt"):
+        assert _read(prefix + ext) == _read(gold + ext), ext
