@@ -222,6 +222,8 @@ def extra_results(which):
         out["long_pairs"] = workloads.run_long(dtypes=())
     if which == "round":
         out["dba_round"] = workloads.run_round()
+    if which == "long_small":
+        out["long_pairs"] = workloads.run_long(len_lo=20_000, len_hi=40_000, with_round=False)
     return out
 
 
@@ -254,18 +256,20 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--n-series", type=int, default=N_SERIES,
                     help="development only: fewer series than the benchmark configuration")
-    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "long", "long_round", "round", "all"],
+    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "long", "long_round", "long_small", "round",
+                             "all"],
                     help="medoid: the metric's configuration (default); batched: many DBA jobs, "
                          "batched vs plain; serving: Poisson request stream, served vs plain; "
                          "long: 16 series of 1M-4M samples, segmentation then all-vs-all f32 and "
                          "f64 and one stripe-mode DBA round (several minutes); long_round: the "
                          "segmentation and the DBA round only; round: one full-path DBA round of 400 "
-                         "members of 3k-8k samples; all: the medoid line with batched and serving added")
+                         "members of 3k-8k samples; long_small: the long workload's all-vs-all "
+                         "with 20k-40k samples (a profiling case); all: the medoid line with batched and serving added")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
-    if args.workload in ("batched", "serving", "long", "long_round", "round"):
+    if args.workload in ("batched", "serving", "long", "long_round", "long_small", "round"):
         return run_extra(args, world, rank, local)
 
     import torch

@@ -22,9 +22,12 @@ namespace odba {
 
 // One cell with its move.  top: open-end top row (right free); fd: the
 // reference's swath-left column on that row (diagonal free too).
-template <typename T, bool MASKED>
+// One cell with its move code already shifted into place: the code of
+// register j sits at bit 2*(j % 16) of the 32-bit half word j / 16, so the
+// two selects take the shifted constants and no shift is needed.
+template <typename T, bool MASKED, int J>
 __device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool fd,
-                                       unsigned &code) {
+                                       unsigned &bits) {
   const T uv = Num<T>::cell(d, up);
   T dv = Num<T>::cell(d, diag);
   T rv = Num<T>::cell(d, left);
@@ -33,9 +36,53 @@ __device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool
     dv = (top && fd) ? diag : dv;
   }
   const T v = Num<T>::min3(uv, dv, rv);
-  code = (dv == v) ? 1u : ((uv == v) ? 3u : 2u);
+  constexpr int sh = 2 * (J % 16);
+  bits = (dv == v) ? (1u << sh) : ((uv == v) ? (3u << sh) : (2u << sh));
   return v;
 }
+
+template <typename T, int R, bool MASKED, int J = 0>
+struct PathCols {
+  // Columns J.. of one step: cells of rows a and b, the codes of two
+  // consecutive columns joined by one three-input OR per half word.
+  static __device__ __forceinline__ void run(T (&col)[R], const T (&yv)[R], T xa, T xb, T &a_left,
+                                             T &a_diag, T &b_left, T &b_diag, bool act_a,
+                                             bool act_b, bool top_a, bool top_b, bool fd0,
+                                             unsigned (&wa)[2], unsigned (&wb)[2]) {
+    if constexpr (J < R) {
+      unsigned ca0, cb0, ca1 = 0, cb1 = 0;
+      {
+        const T up = col[J];
+        T va = path_cell<T, MASKED, J>(xa - yv[J], up, a_diag, a_left, top_a, J == 0 && fd0, ca0);
+        if (MASKED) va = act_a ? va : up;
+        a_diag = up;
+        a_left = va;
+        T vb = path_cell<T, MASKED, J>(xb - yv[J], va, b_diag, b_left, top_b, J == 0 && fd0, cb0);
+        if (MASKED) vb = act_b ? vb : va;
+        b_diag = va;
+        b_left = vb;
+        col[J] = vb;
+      }
+      if constexpr (J + 1 < R) {
+        const T up = col[J + 1];
+        T va = path_cell<T, MASKED, J + 1>(xa - yv[J + 1], up, a_diag, a_left, top_a, false, ca1);
+        if (MASKED) va = act_a ? va : up;
+        a_diag = up;
+        a_left = va;
+        T vb = path_cell<T, MASKED, J + 1>(xb - yv[J + 1], va, b_diag, b_left, top_b, false, cb1);
+        if (MASKED) vb = act_b ? vb : va;
+        b_diag = va;
+        b_left = vb;
+        col[J + 1] = vb;
+      }
+      constexpr int h = (J % 32) / 16;  // J and J + 1 share a half word (J even)
+      wa[h] = wa[h] | ca0 | ca1;
+      wb[h] = wb[h] | cb0 | cb1;
+      PathCols<T, R, MASKED, J + 2>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a,
+                                         act_b, top_a, top_b, fd0, wa, wb);
+    }
+  }
+};
 
 template <typename T, int R, bool MASKED>
 __device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa, T xb, T la,
@@ -44,24 +91,11 @@ __device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa
                                              unsigned long long &wb) {
   T a_left = la, a_diag = dg;
   T b_left = lb, b_diag = la;
-  wa = 0ull;
-  wb = 0ull;
-#pragma unroll
-  for (int j = 0; j < R; ++j) {
-    const T up = col[j];
-    unsigned ca, cb;
-    T va = path_cell<T, MASKED>(xa - yv[j], up, a_diag, a_left, top_a, j == 0 && fd0, ca);
-    if (MASKED) va = act_a ? va : up;
-    a_diag = up;
-    a_left = va;
-    T vb = path_cell<T, MASKED>(xb - yv[j], va, b_diag, b_left, top_b, j == 0 && fd0, cb);
-    if (MASKED) vb = act_b ? vb : va;
-    b_diag = va;
-    b_left = vb;
-    col[j] = vb;
-    wa |= (unsigned long long)ca << (2 * j);
-    wb |= (unsigned long long)cb << (2 * j);
-  }
+  unsigned ha[2] = {0u, 0u}, hb[2] = {0u, 0u};
+  PathCols<T, R, MASKED, 0>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a, act_b,
+                                 top_a, top_b, fd0, ha, hb);
+  wa = (unsigned long long)ha[0] | ((unsigned long long)ha[1] << 32);
+  wb = (unsigned long long)hb[0] | ((unsigned long long)hb[1] << 32);
   return a_left;
 }
 
