@@ -128,8 +128,20 @@ size_t round_workspace(const uint64_t *lens, int n, uint64_t Lc, int os, int oe,
     cudaGetLastError();
   }
   if (!stripe) return full;
+  // tile height: ODBA_STRIPE_ROWS, else the smallest of 1024, 2048, ... whose
+  // workspace fits in free memory (shorter tiles recompute with more warps
+  // at once: 16 x 1M-4M members, 4096 rows 97 s, 1024 rows 75 s per round)
   int rows = 0;
   if (const char *r = std::getenv("ODBA_STRIPE_ROWS")) rows = std::atoi(r);
+  if (rows <= 0) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+    cudaGetLastError();
+    rows = 1024;
+    while (rows < (1 << 20) &&
+           odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, rows) > fr / 20 * 19)
+      rows *= 2;
+  }
   *stripe_rows = rows;
   return odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, rows);
 }

@@ -250,18 +250,21 @@ def _long_round(raw):
     L = np.array([len(s) for s in raw], dtype=np.float64)
     h = np.ascontiguousarray(ds.host_lens, dtype=np.uint64)
     lib = _native.lib()
-    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0, 0)
+    import os
+    rows = int(os.environ.get("ODBA_STRIPE_ROWS", "1024"))
+    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0, rows)
     ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     a.record()
-    mean, counts, delta, _ = api.dba_round(cen, ds, 0, 0, workspace=ws, stripe_rows=0)
+    mean, counts, delta, _ = api.dba_round(cen, ds, 0, 0, workspace=ws, stripe_rows=rows)
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
     cells = float(L.sum()) * len(cen)
     full_path_tb = float(L.sum()) * len(cen) / 4 / 1e12
-    return {"centroid_len": len(cen), "members": len(raw), "seconds": ms / 1e3,
+    return {"centroid_len": len(cen), "members": len(raw), "tile_rows": rows or 4096,
+            "seconds": ms / 1e3,
             "forward_cells": cells, "gcups": cells / ms / 1e6, "workspace_gb": nbytes / 1e9,
             "full_path_would_need_tb": full_path_tb, "delta": float(delta),
             "finite_mean": bool(torch.isfinite(mean).all().item())}
