@@ -219,7 +219,10 @@ int odba_znorm_f64(double *series, const uint64_t *offsets, const uint64_t *lens
  * member k starting at triple sum_{i<k}(lens[i] + Lc + 1), the path as
  * (row, column, move) int32 triples in the order of the reference's path file
  * (io_utils.hpp:287-323, move codes of dtw.hpp:10-16), and path_counts[k] the
- * number of triples (-1 if the walk failed). */
+ * number of triples (-1 if the walk failed).  The path DTW may run as a swath
+ * pipeline whose hand-off waits are bounded: if one ever runs out, the 32-bit
+ * word at byte 8 of the workspace is non-zero after the round (it is cleared
+ * at every launch; the same holds for the batched and stripe-mode rounds). */
 size_t odba_dba_round_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
                                       uint64_t centroid_len, int use_open_start, int use_open_end);
 int odba_dba_round_f32(const float *centroid, uint64_t centroid_len, const float *series,
@@ -406,7 +409,8 @@ int odba_segment_host_f64(const double *h_series, const uint64_t *h_lens, int n,
  * same results.  Outputs per job: h_medoids[j] (index within the job's input
  * order), its centroid at h_centroids[h_centroid_offsets[j]] with the medoid's
  * length (capacity: the sum over jobs of the longest series), rounds run and
- * the last delta.  max_rounds <= 0 means the reference's 250. */
+ * the last delta.  max_rounds <= 0 means the reference's 250.  Returns
+ * ODBA_ERR_TIMEOUT if a swath hand-off wait ran out on the device. */
 int odba_dba_jobs_f32(const float *h_series, const uint64_t *h_lens, const int *job_begin,
                       const int *job_end, const int *job_flags, int njobs, int norm,
                       int max_rounds, int batched, int *h_medoids, uint64_t *h_centroid_offsets,

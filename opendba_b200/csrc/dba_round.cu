@@ -1257,7 +1257,9 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
   sa.q_stride = S.q_stride;
   sa.prog = reinterpret_cast<unsigned long long *>(base + S.off_prog);
   sa.counter = reinterpret_cast<unsigned long long *>(head);
-  sa.err = reinterpret_cast<unsigned *>(head + 8);
+  // the wait error word is byte 8 of the workspace, as in the full-path round
+  sa.err = reinterpret_cast<unsigned *>(base + L.off_counter + 8);
+  cudaMemsetAsync(base + L.off_counter, 0, 16, stream);
   sa.walk = reinterpret_cast<StripeWalk *>(head + 64);
   sa.words = reinterpret_cast<unsigned long long *>(base + S.off_W);
   sa.limit_ns = kWaitLimitNs;

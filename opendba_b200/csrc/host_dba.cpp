@@ -146,6 +146,24 @@ size_t round_workspace(const uint64_t *lens, int n, uint64_t Lc, int os, int oe,
   return odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, rows);
 }
 
+// True if the launch that used workspace ws (pairwise or round) reported a
+// swath hand-off wait that ran out: the error word at byte 8, which every
+// launch clears.  Call after the launch's stream has synchronized.
+bool wait_ran_out(const void *ws) {
+  unsigned err = 0;
+  check_cuda(cudaMemcpy(&err, static_cast<const char *>(ws) + 8, sizeof err, cudaMemcpyDeviceToHost),
+             "wait error word");
+  return err != 0;
+}
+
+// The pipeline's form: ends the process like the other device errors.
+void check_wait(const void *ws, const char *what) {
+  if (wait_ran_out(ws)) {
+    std::cerr << what << ": a swath hand-off wait ran out on the device" << std::endl;
+    die(odba_exit::DEVICE_LIBRARY_ERROR);
+  }
+}
+
 // RAII device buffer.
 struct DevBuf {
   void *p = nullptr;
@@ -398,6 +416,7 @@ int *medoid_pass(const T *d_data, const uint64_t *d_offs, const uint64_t *d_lens
     check_cuda(cudaMemcpyAsync(dists.data(), d_dists.p, npairs * sizeof(T), cudaMemcpyDeviceToHost, st),
                "distance download");
     check_cuda(cudaStreamSynchronize(st), "all-pairs DTW");
+    check_wait(ws.p, "all-pairs DTW");
   }
   std::vector<T> sos(n, T(0));
   T max_distance = T(0);
@@ -482,6 +501,7 @@ std::vector<T> converge_cluster(const DeviceSet<T> &all, const std::vector<int> 
     check_cuda(cudaMemcpyAsync(nb.data(), d_mean.p, Lc * sizeof(T), cudaMemcpyDeviceToHost, st), "centroid download");
     check_cuda(cudaMemcpyAsync(&delta, d_delta.p, sizeof(double), cudaMemcpyDeviceToHost, st), "delta download");
     check_cuda(cudaStreamSynchronize(st), "DBA round");
+    check_wait(ws.p, "DBA round");
     std::cerr << "New delta is " << delta << std::endl;
     if (delta == 0) break;
     if (os || oe) {
@@ -601,6 +621,7 @@ double DBAUpdate(T *C, size_t centerLength, T **sequences, char **sequence_names
   check_cuda(cudaMemcpyAsync(updatedMean, d_mean.p, centerLength * sizeof(T), cudaMemcpyDefault, stream), "centroid download");
   check_cuda(cudaMemcpyAsync(&delta, d_delta.p, sizeof(double), cudaMemcpyDeviceToHost, stream), "delta download");
   check_cuda(cudaStreamSynchronize(stream), "DBA round");
+  check_wait(ws.p, "DBA round");
   if (!output_prefix.empty()) {
     std::vector<int64_t> tc(n);
     std::vector<int32_t> tri(3 * cap);
@@ -1472,6 +1493,7 @@ int run_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, co
                                         ws.bytes, st),
             "pair-list DTW");
     check_cuda(cudaStreamSynchronize(st), "pair-list DTW");
+    if (wait_ran_out(ws.p)) return ODBA_ERR_TIMEOUT;
   }
   for (int j = 0; j < njobs; ++j) {
     const int b = js.jbeg[j], m = js.jend[j] - js.jbeg[j];
@@ -1487,7 +1509,10 @@ int run_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, co
               : odba_medoid_f64((const double *)d_dists.p + tri_off[j], ptr<uint64_t>(js.ds.lens) + b,
                                 m, (double *)d_sos.p + b, ptr<int>(d_med) + j, st),
           "medoid");
-    if (!batched) check_cuda(cudaStreamSynchronize(st), "medoid");
+    if (!batched) {
+      check_cuda(cudaStreamSynchronize(st), "medoid");
+      if (m >= 2 && wait_ran_out(ws.p)) return ODBA_ERR_TIMEOUT;
+    }
   }
   std::vector<int> med(njobs, 0);
   check_cuda(cudaMemcpyAsync(med.data(), d_med.p, njobs * sizeof(int), cudaMemcpyDeviceToHost, st), "medoid download");
@@ -1648,6 +1673,10 @@ int run_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, co
         check_cuda(cudaMemcpyAsync(nb.data(), cbuf[1 - cur].p, ctot * sizeof(T), cudaMemcpyDeviceToHost, st), "means");
         check_cuda(cudaMemcpyAsync(deltas.data(), d_deltas.p, njobs * sizeof(double), cudaMemcpyDeviceToHost, st), "deltas");
         check_cuda(cudaStreamSynchronize(st), "batched round");
+        if (wait_ran_out(rws.p)) {
+          for (int g = 0; g < 2; ++g) cudaGraphExecDestroy(exec[g]);
+          return ODBA_ERR_TIMEOUT;
+        }
         for (int j = 0; j < njobs; ++j) {
           if (!active[j]) continue;
           rounds[j] = round + 1;
@@ -1686,6 +1715,7 @@ int run_jobs(const T *h_series, const uint64_t *h_lens, const int *job_begin, co
         check_cuda(cudaMemcpyAsync(v.data(), cout, clen[j] * sizeof(T), cudaMemcpyDeviceToHost, st), "means");
         check_cuda(cudaMemcpyAsync(&delta, ptr<double>(d_deltas) + j, sizeof(double), cudaMemcpyDeviceToHost, st), "delta");
         check_cuda(cudaStreamSynchronize(st), "DBA round");
+        if (wait_ran_out(rws.p)) return ODBA_ERR_TIMEOUT;
         rounds[j] = round + 1;
         h_deltas[j] = delta;
         std::copy(v.begin(), v.end(), host_c.begin() + coff[j]);

@@ -467,6 +467,9 @@ class Server {
         for (auto &r : medoid_jobs)
           ServerOps<T>::medoid(r->d_dists, r->d_lens, int(r->lens.size()), r->d_sos, r->d_med, st_);
       }
+      // the pair kernels' hand-off wait error word (byte 8 of the workspace)
+      unsigned wait_err = 0;
+      if (ok) cudaMemcpyAsync(&wait_err, static_cast<char *>(ws) + 8, sizeof wait_err, cudaMemcpyDeviceToHost, st_);
       cudaFreeAsync(d_tasks, st_);
       cudaFreeAsync(d_offs, st_);
       cudaFreeAsync(d_lens, st_);
@@ -475,6 +478,10 @@ class Server {
       if (!ok || cudaStreamSynchronize(st_) != cudaSuccess) {
         cudaGetLastError();
         for (auto &o : outs) finish(o.first, kFailed, ODBA_ERR_CUDA);
+        return;
+      }
+      if (wait_err) {
+        for (auto &o : outs) finish(o.first, kFailed, ODBA_ERR_TIMEOUT);
         return;
       }
       cells_ += cells;
@@ -588,14 +595,21 @@ class Server {
         static_cast<int32_t *>(nullptr), static_cast<int64_t *>(nullptr), blob + o[14], wsb, st_);
     std::vector<T> nb(ctot);
     std::vector<double> deltas(nj);
+    unsigned wait_err = 0;
     if (rc == ODBA_OK) {
       cudaMemcpyAsync(nb.data(), blob + o[1], ctot * sizeof(T), cudaMemcpyDeviceToHost, st_);
       cudaMemcpyAsync(deltas.data(), blob + o[3], nj * 8, cudaMemcpyDeviceToHost, st_);
+      // the round's hand-off wait error word (byte 8 of its workspace)
+      cudaMemcpyAsync(&wait_err, blob + o[14] + 8, sizeof wait_err, cudaMemcpyDeviceToHost, st_);
     }
     cudaFreeAsync(blob, st_);
     if (rc != ODBA_OK || cudaStreamSynchronize(st_) != cudaSuccess) {
       cudaGetLastError();
       for (auto &r : rj) finish(r, kFailed, ODBA_ERR_CUDA);
+      return;
+    }
+    if (wait_err) {
+      for (auto &r : rj) finish(r, kFailed, ODBA_ERR_TIMEOUT);
       return;
     }
     cells_ += rcells;
