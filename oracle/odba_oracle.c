@@ -13,6 +13,7 @@
  *   backtrack / centroid pile-up                dba.hpp:374-423
  *   DBA round mean and delta                    dba.hpp:817-836
  *   path file line order                        io_utils.hpp:287-323
+ *   stripe-mode round (odba_stripe.inc)         dba.hpp:515-763, dtw.hpp:74-239
  *   z-normalisation                             gpu_utils.hpp:34-170
  */
 #include "odba_oracle.h"
@@ -32,6 +33,21 @@
 static const int kMoveI[7] = {-1, -1, 0, -1, 0, 0, 0}; /* dtw.hpp:20 */
 static const int kMoveJ[7] = {-1, -1, -1, 0, -1, -1, -1}; /* dtw.hpp:21 */
 
+/* The open-end shortcut's column minimum (dtw.hpp:83-105) is read from one
+ * shared word that all 32 lanes of warp 0 store their partial minimum to; lane
+ * l's partial covers the rows r with r % 1024 >= 32*l.  On the B200 the
+ * reference's float build reads lane 0's store (the full minimum) and its
+ * double build lane 16's (rows with r % 1024 >= 512), as its stripe-mode and
+ * open-end runs show (tests/golden/ref/stripe_*). */
+static int g_shortcut_lane[2] = {0, 16}; /* float, double */
+#define SHORTCUT_LANE_f32 g_shortcut_lane[0]
+#define SHORTCUT_LANE_f64 g_shortcut_lane[1]
+
+void oracle_set_shortcut_lanes(int lane_f32, int lane_f64) {
+  g_shortcut_lane[0] = lane_f32;
+  g_shortcut_lane[1] = lane_f64;
+}
+
 #define DEFINE_ORACLE(T, SFX, FMA, TMAX)                                                        \
   static inline T add_dd_##SFX(T acc, T d, int fma_mode) {                                     \
     if (fma_mode) return FMA(d, d, acc);                                                       \
@@ -39,10 +55,11 @@ static const int kMoveJ[7] = {-1, -1, -1, 0, -1, -1, -1}; /* dtw.hpp:21 */
     return acc + dd;                                                                           \
   }                                                                                            \
                                                                                                \
-  /* Full cost matrix sweep, row by row.  Keeps two rows; optionally stores moves and the     \
-   * per-swath-boundary column minima the open-end shortcut needs.  Returns C[m-1][n-1]. */    \
+  /* Full cost matrix sweep, row by row.  Keeps two rows; optionally stores moves, every    \
+   * cost (costs[r*n+c]) and the per-swath-boundary column minima the open-end shortcut      \
+   * needs.  Returns C[m-1][n-1]. */                                                           \
   static T sweep_##SFX(const T *first, size_t m, const T *second, size_t n, int os, int oe,     \
-                       int fma_mode, unsigned char *path, T *bmin, T *btop) {                  \
+                       int fma_mode, unsigned char *path, T *bmin, T *btop, T *costs) {        \
     T *prev = (T *)malloc(sizeof(T) * n);                                                      \
     T *cur = (T *)malloc(sizeof(T) * n);                                                       \
     size_t nb = n / SWATH + 1;                                                                 \
@@ -105,9 +122,10 @@ static const int kMoveJ[7] = {-1, -1, -1, 0, -1, -1, -1}; /* dtw.hpp:21 */
         }                                                                                      \
         cur[c] = v;                                                                            \
         if (path) path[r * n + c] = mv;                                                        \
+        if (costs) costs[r * n + c] = v;                                                       \
         if (bmin && (c + 1) % SWATH == 0) {                                                    \
           size_t k = (c + 1) / SWATH;                                                          \
-          if (v < bmin[k]) bmin[k] = v;                                                        \
+          if ((r % SWATH) >= (size_t)(32 * SHORTCUT_LANE_##SFX) && v < bmin[k]) bmin[k] = v;   \
           if (r == m - 1) btop[k] = v;                                                         \
         }                                                                                      \
       }                                                                                        \
@@ -137,25 +155,24 @@ static const int kMoveJ[7] = {-1, -1, -1, 0, -1, -1, -1}; /* dtw.hpp:21 */
                             int oe, int fma_mode, T *dist_out, unsigned char *path) {          \
     if (m == 0 || n == 0) return -1;                                                           \
     size_t nb = n / SWATH + 1;                                                                 \
-    T *bmin = NULL, *btop = NULL;                                                              \
-    if (path) {                                                                                \
-      bmin = (T *)malloc(sizeof(T) * nb);                                                      \
-      btop = (T *)calloc(nb, sizeof(T));                                                       \
-    }                                                                                          \
-    T last = sweep_##SFX(first, m, second, n, os, oe, fma_mode, path, bmin, btop);             \
-    if (path) {                                                                                \
-      size_t c0 = shortcut_col_##SFX(m, n, os, oe, bmin, btop);                                \
-      if (c0)                                                                                  \
-        for (size_t c = c0; c < n; ++c) path[(m - 1) * n + c] = ORACLE_OPEN_RIGHT;             \
-      free(bmin);                                                                              \
-      free(btop);                                                                              \
-    }                                                                                          \
+    T *bmin = (T *)malloc(sizeof(T) * nb);                                                     \
+    T *btop = (T *)calloc(nb, sizeof(T));                                                      \
+    T last = sweep_##SFX(first, m, second, n, os, oe, fma_mode, path, bmin, btop, NULL);       \
+    size_t c0 = shortcut_col_##SFX(m, n, os, oe, bmin, btop);                                  \
+    if (path && c0)                                                                            \
+      for (size_t c = c0; c < n; ++c) path[(m - 1) * n + c] = ORACLE_OPEN_RIGHT;               \
+    const T frozen = c0 ? btop[c0 / SWATH] : (T)0;                                             \
+    free(bmin);                                                                                \
+    free(btop);                                                                                \
     if (dist_out) {                                                                            \
-      /* The shortcut never changes the top-row value it freezes, so the distance is the     \
-       * full sweep's corner -- except for a single-row matrix, where the shortcut reads the \
-       * sentinel it has just written (dtw.hpp:113, 121). */                                   \
-      if (m == 1 && oe && !os && n > SWATH) {                                                  \
+      /* Where the shortcut fires the distance is the top-row value it freezes (dtw.hpp:113,  \
+       * 121): the full sweep's corner when its minimum covers the whole column, but not     \
+       * always with the double build's partial minimum; a single-row matrix reads the       \
+       * sentinel it has just written. */                                                      \
+      if (c0 && m == 1) {                                                                      \
         *dist_out = (T)(sqrtf((float)TMAX) / (float)m);                                        \
+      } else if (c0) {                                                                         \
+        *dist_out = (T)(sqrtf((float)frozen) / (float)m);                                      \
       } else if ((oe && !os) || (!oe && os)) {                                                 \
         *dist_out = (T)(sqrtf((float)last) / (float)m);                                        \
       } else {                                                                                 \
@@ -330,6 +347,22 @@ static double warp_tree_dbl(double *v) {
 
 DEFINE_ORACLE(float, f32, fmaf, FLT_MAX)
 DEFINE_ORACLE(double, f64, fma, DBL_MAX)
+
+/* stripe-mode DBA round (dba.hpp:515-763), once per value type */
+#define ST float
+#define SNAME(x) x##_f32
+#define STMAX FLT_MAX
+#include "odba_stripe.inc"
+#undef ST
+#undef SNAME
+#undef STMAX
+#define ST double
+#define SNAME(x) x##_f64
+#define STMAX DBL_MAX
+#include "odba_stripe.inc"
+#undef ST
+#undef SNAME
+#undef STMAX
 
 #define DEFINE_ZNORM(T, SFX)                                                                   \
   int oracle_znorm_##SFX(T *series, const uint64_t *offsets, const uint64_t *lens, int n,      \

@@ -27,6 +27,11 @@ extern "C" {
 #define ORACLE_OPEN_RIGHT 4
 #define ORACLE_NIL_OPEN_RIGHT 5
 
+/* Which warp-0 lane's partial minimum the open-end shortcut check reads in
+ * the float and double restatements (defaults 0 and 16, the reference's B200
+ * builds); tests vary it to find inputs that tell lanes apart. */
+void oracle_set_shortcut_lanes(int lane_f32, int lane_f64);
+
 /* One pair: first (rows, length m) against second (columns, length n).
  * dist_out receives the reference's medoid-pass distance (dtw.hpp:116-125,
  * 242-257).  If path is non-NULL it receives m*n move codes, row-major
@@ -77,6 +82,24 @@ double oracle_dba_update_f64(const double *centroid, size_t Lc, const double *se
                              const uint64_t *offsets, const uint64_t *lens, int n,
                              int open_start, int open_end, int fma_mode, double *mean_out,
                              uint32_t *counts_out, double *sums_out);
+
+/* One DBA round in the reference's stripe mode (dba.hpp:515-763), including
+ * the open-end rules its stripe re-run applies at the backtrack height (see
+ * odba_stripe.inc).  lane: which warp-0 lane's partial minimum the open-end
+ * shortcut check reads (0: the full minimum).  Per-member path cells
+ * (row, column, move) go to triples back to back (tri_counts[k] cells for
+ * member k, -1 if tri_cap ran out); hazards[k] counts the walk's stripe exits
+ * on row 0 past the first stripe. */
+double oracle_dba_update_stripe_f32(const float *centroid, size_t Lc, const float *series,
+                                    const uint64_t *offsets, const uint64_t *lens, int n,
+                                    int open_start, int open_end, int fma_mode, int lane,
+                                    float *mean_out, uint32_t *counts_out, int64_t *triples,
+                                    int64_t tri_cap, int64_t *tri_counts, int64_t *hazards);
+double oracle_dba_update_stripe_f64(const double *centroid, size_t Lc, const double *series,
+                                    const uint64_t *offsets, const uint64_t *lens, int n,
+                                    int open_start, int open_end, int fma_mode, int lane,
+                                    double *mean_out, uint32_t *counts_out, int64_t *triples,
+                                    int64_t tri_cap, int64_t *tri_counts, int64_t *hazards);
 
 /* Backtrack of one member against the centroid, emitting the (i, j, move)
  * triples in the order the reference's path file lists them (io_utils.hpp:287-323),

@@ -55,6 +55,13 @@ def lib():
             f.argtypes = [P, ctypes.c_size_t, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                           ctypes.c_int, P, P, P]
             f.restype = ctypes.c_double
+            f = _lib.oracle_set_shortcut_lanes
+            f.argtypes = [ctypes.c_int, ctypes.c_int]
+            f.restype = None
+            f = getattr(_lib, f"oracle_dba_update_stripe_{sfx}")
+            f.argtypes = [P, ctypes.c_size_t, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                          ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_int64, P, P]
+            f.restype = ctypes.c_double
             f = getattr(_lib, f"oracle_path_triples_{sfx}")
             f.argtypes = [P, ctypes.c_size_t, P, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                           ctypes.c_int, P, ctypes.c_int64]
@@ -147,6 +154,46 @@ def dba_update(centroid, members, open_start=0, open_end=0, fma_mode=1):
         _ptr(centroid), Lc, _ptr(flat), _ptr(offsets), _ptr(lens), len(members), open_start,
         open_end, fma_mode, _ptr(mean), _ptr(counts), _ptr(sums))
     return mean, counts, sums, delta
+
+
+# which warp-0 lane's partial minimum the reference's open-end shortcut reads
+# (dtw.hpp:97-105): lane 0 (the full minimum) in its float build, lane 16 in
+# its double build, pinned by its stripe-mode runs (tests/golden/ref/stripe_*)
+SHORTCUT_LANE = {np.dtype(np.float32): 0, np.dtype(np.float64): 16}
+
+
+def set_shortcut_lanes(lane_f32=0, lane_f64=16):
+    """Which lane's partial minimum the open-end shortcut reads (see
+    SHORTCUT_LANE); the defaults are the reference's."""
+    lib().oracle_set_shortcut_lanes(lane_f32, lane_f64)
+
+
+def dba_update_stripe(centroid, members, open_start=0, open_end=0, fma_mode=1, lane=None):
+    """One DBA round in the reference's stripe mode (dba.hpp:515-763), with the
+    open-end rules its stripe re-run applies at the backtrack height.  Returns
+    (mean, counts, delta, paths, hazards): paths[k] is member k's (row, column,
+    move) cells in walk order, hazards[k] its walk's row-0 stripe exits."""
+    centroid = np.ascontiguousarray(centroid)
+    if lane is None:
+        lane = SHORTCUT_LANE[centroid.dtype]
+    flat, offsets, lens = pack(members, centroid.dtype)
+    Lc = len(centroid)
+    mean = np.zeros(Lc, dtype=centroid.dtype)
+    counts = np.zeros(Lc, dtype=np.uint32)
+    n = len(members)
+    cap = int(sum(Lc + len(x) + 2 for x in members))
+    tri = np.zeros(3 * cap, dtype=np.int64)
+    tcnt = np.zeros(n, dtype=np.int64)
+    hz = np.zeros(n, dtype=np.int64)
+    delta = getattr(lib(), f"oracle_dba_update_stripe_{_sfx(centroid.dtype)}")(
+        _ptr(centroid), Lc, _ptr(flat), _ptr(offsets), _ptr(lens), n, open_start, open_end,
+        fma_mode, lane, _ptr(mean), _ptr(counts), _ptr(tri), cap, _ptr(tcnt), _ptr(hz))
+    assert (tcnt >= 0).all()
+    paths, o = [], 0
+    for k in range(n):
+        paths.append(tri[3 * o:3 * (o + tcnt[k])].reshape(-1, 3))
+        o += int(tcnt[k])
+    return mean, counts, delta, paths, hz
 
 
 def path_triples(centroid, seq, open_start=0, open_end=0, fma_mode=1):

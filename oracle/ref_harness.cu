@@ -19,7 +19,9 @@
 //   dbaupdate  <members.odbs> <centroid.odbs> <out_prefix> <open_start> <open_end>
 //       One DBAUpdate round (dba.hpp:432-848): writes <out_prefix>.mean.odbs
 //       (the updated centroid), <out_prefix>.delta.txt and the per-member
-//       path files <out_prefix>.path<k>.txt.
+//       path files <out_prefix>.path<k>.txt.  With the environment variable
+//       ODBA_HARNESS_FORCE_STRIPE set, the round runs in the reference's stripe
+//       mode (dba.hpp:515-763).
 //   znorm      <in.odbs> <out_prefix>
 //       normalizeSequences (gpu_utils.hpp:132-170): writes the normalised
 //       series, and the per-series means and sigmas (float64).
@@ -37,6 +39,20 @@
 #include <fstream>
 #include <string>
 #include <vector>
+
+#include <cuda_runtime.h>
+
+// Forced stripe mode (dbaupdate with ODBA_HARNESS_FORCE_STRIPE set): DBAUpdate
+// takes its stripe path when the free device memory it reads is below the full
+// path matrix's size (dba.hpp:523-525), so the harness reports no free memory
+// to the reference's code while the flag is on.
+static bool g_force_stripe = false;
+static cudaError_t harness_mem_get_info(size_t *free_bytes, size_t *total_bytes) {
+  const cudaError_t e = cudaMemGetInfo(free_bytes, total_bytes);
+  if (g_force_stripe && free_bytes) *free_bytes = 0;
+  return e;
+}
+#define cudaMemGetInfo harness_mem_get_info
 
 #include "openDBA.cuh"
 #include "series_bundle.h"
@@ -256,6 +272,7 @@ static int run_segment(const SeriesBundle &b, const std::string &out, int minseg
 int main(int argc, char **argv) {
   if (argc < 3) die("usage: ref_harness <mode> args...");
   std::string mode = argv[1];
+  g_force_stripe = mode == "dbaupdate" && std::getenv("ODBA_HARNESS_FORCE_STRIPE") != nullptr;
   int rc = 0;
   if (mode == "setupandrun") {
     if (argc < 7) die("setupandrun <prefix> <os> <oe> <norm> <files...>");

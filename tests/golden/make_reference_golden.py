@@ -7,7 +7,8 @@ committed copy lives in tests/golden/ref/; tests compare the CUDA path and
 the CPU oracle against it.
 
 Run on a B200 box from the repository root:
-    python tests/golden/make_reference_golden.py [out_dir] [--clusters-only | --chop-only]
+    python tests/golden/make_reference_golden.py [out_dir] [--clusters-only | --chop-only |
+                                                           --stripe-only | --shortcut-only]
 """
 from __future__ import annotations
 
@@ -32,9 +33,10 @@ MODES = {"global": (0, 0), "open_start": (1, 0), "open_end": (0, 1), "open": (1,
 FIXTURES = "tests/golden/ref_fixtures"
 
 
-def run(args, log, cwd=None):
+def run(args, log, cwd=None, env=None):
     t0 = time.time()
-    p = subprocess.run([HARNESS] + [str(a) for a in args], capture_output=True, text=True, cwd=cwd)
+    p = subprocess.run([HARNESS] + [str(a) for a in args], capture_output=True, text=True, cwd=cwd,
+                       env=env)
     log.write(json.dumps({"args": [str(a) for a in args], "rc": p.returncode,
                           "secs": round(time.time() - t0, 3), "stdout": p.stdout[-2000:],
                           "stderr": p.stderr[-2000:]}) + "\n")
@@ -156,6 +158,153 @@ def cluster_cases(out, tmp, log):
                 shutil.copy(pfx + ext, os.path.join(out, name + ext))
 
 
+def warped_copy(rng, base, L, noise):
+    """base resampled to L samples along a random monotone time warp, plus
+    N(0, noise) noise, z-normalised."""
+    w = np.cumsum(rng.uniform(0.3, 1.7, L))
+    w = (w - w[0]) / (w[-1] - w[0]) * (len(base) - 1)
+    x = np.interp(w, np.arange(len(base)), base) + rng.normal(0, noise, L)
+    return (x - x.mean()) / x.std()
+
+
+# stripe-mode sets: seed offset, centroid length, member lengths (shorter and
+# longer than the centroid, so both orientations of the open-end flip occur)
+STRIPE_SETS = {"a": (606, 2300, [1500, 2100, 2900, 3600, 4700, 5200, 2400, 1900]),
+               "b": (607, 1800, [1200, 2500, 3900, 6100, 1790, 2950, 4400, 800]),
+               "c": (608, 3100, [2000, 3300, 5000, 7000, 2600, 4100]),
+               "d": (616, 2600, [1700, 3000, 4300, 5600, 2200, 3500, 6400, 2500]),
+               "e": (704, 2835, [5602, 5527, 1051, 1367, 2651, 3002, 5156, 1361]),
+               "f": (713, 3064, [3040, 4863, 1153, 5175, 6223, 2152, 6333, 1267]),
+               "g": (708, 2626, [4473, 3479, 2927, 4931, 5622, 3683, 6785, 5564]),
+               "h": (719, 3326, [6668, 3906, 3632, 5977, 2595, 3609, 3562, 5240])}
+
+
+def stripe_inputs(dtype, tag):
+    seed, Lc, lens = STRIPE_SETS[tag]
+    rng = np.random.default_rng(synth.SEED_BASE + seed)
+    base = synth.step_signal(rng, Lc, 90.0, 12.0, 10.0, 2.0).astype(np.float64)
+    base = (base - base.mean()) / base.std()
+    members = [warped_copy(rng, base, L, 0.3).astype(dtype) for L in lens]
+    return base.astype(dtype), members
+
+
+def stripe_safe(centroid, members, os_, oe):
+    """True if no walk of the oracle's stripe restatement leaves a stripe past
+    the first on row 0, whichever warp-0 lane the shortcut check reads: there
+    the reference's stripe walk reads one byte before its stripe path buffer
+    (dba.hpp:403 with j = -1, i = 0)."""
+    lanes = range(32) if (oe and not os_) else (0,)
+    return all(not O.dba_update_stripe(centroid, members, os_, oe, lane=lane)[4].any()
+               for lane in lanes)
+
+
+def _sha(b: bytes) -> str:
+    import hashlib
+    return hashlib.sha256(b).hexdigest()
+
+
+def path_digest(ij: np.ndarray, mv: np.ndarray) -> str:
+    """sha256 of one path listing: (row, column) as int32 pairs, then moves as bytes."""
+    return _sha(np.ascontiguousarray(ij, dtype=np.int32).tobytes() +
+                np.ascontiguousarray(mv, dtype=np.uint8).tobytes())
+
+
+def stripe_summary(out):
+    """Digests of the stripe-mode outputs (stripe_ref.json): input bundles,
+    mean bytes, delta and every member's path, so the fixtures stay small;
+    set "a" also keeps its raw outputs for diagnosis."""
+    summary = {"sets": {k: list(v) for k, v in STRIPE_SETS.items()}, "inputs": {}, "cases": {}}
+    for tag in STRIPE_SETS:
+        for sfx in ("f32", "f64"):
+            for part in ("members", "centroid"):
+                f = os.path.join(out, f"stripe_{tag}_{sfx}_{part}.odbs")
+                with open(f, "rb") as fh:
+                    summary["inputs"][f"{tag}_{sfx}_{part}"] = _sha(fh.read())
+            for mode in MODES:
+                name = f"stripe_{tag}_{sfx}_{mode}"
+                if not os.path.exists(os.path.join(out, name + ".mean.odbs")):
+                    continue
+                mean = O.read_bundle(os.path.join(out, name + ".mean.odbs"))[0]
+                with open(os.path.join(out, name + ".delta.txt")) as fh:
+                    delta = fh.read().strip()
+                gp = np.load(os.path.join(out, name + ".paths.npz"))
+                paths = []
+                k = 0
+                while f"ij{k}" in gp:
+                    paths.append(path_digest(gp[f"ij{k}"], gp[f"mv{k}"]))
+                    k += 1
+                summary["cases"][f"{tag}_{sfx}_{mode}"] = {
+                    "mean": _sha(mean.tobytes()), "delta": delta, "paths": paths}
+    with open(os.path.join(out, "stripe_ref.json"), "w") as fh:
+        json.dump(summary, fh, indent=1, sort_keys=True)
+
+
+def stripe_cases(out, tmp, log):
+    """One DBAUpdate round in the reference's stripe mode (dba.hpp:515-763),
+    forced by the harness, all four modes, float and double."""
+    env = dict(os.environ, ODBA_HARNESS_FORCE_STRIPE="1")
+    for tag in STRIPE_SETS:
+        for dt, sfx in ((np.float32, "f32"), (np.float64, "f64")):
+            centroid, members = stripe_inputs(dt, tag)
+            mfile = os.path.join(out, f"stripe_{tag}_{sfx}_members.odbs")
+            cfile = os.path.join(out, f"stripe_{tag}_{sfx}_centroid.odbs")
+            O.write_bundle(mfile, members)
+            O.write_bundle(cfile, [centroid])
+            for mode, (os_, oe) in MODES.items():
+                name = f"stripe_{tag}_{sfx}_{mode}"
+                if not stripe_safe(centroid, members, os_, oe):
+                    log.write(json.dumps({"skipped": name, "why": "row-0 stripe exit"}) + "\n")
+                    continue
+                pfx = os.path.join(tmp, name)
+                run(["dbaupdate", mfile, cfile, pfx, os_, oe], log, env=env)
+                for ext in (".mean.odbs", ".delta.txt"):
+                    if os.path.exists(pfx + ext):
+                        shutil.copy(pfx + ext, os.path.join(out, name + ext))
+                paths_to_npz(pfx, os.path.join(out, name + ".paths.npz"))
+
+
+def shortcut_mix_series(dtype):
+    """Lengths around and past 512 rows and a single sample, so that the
+    open-end shortcut (dtw.hpp:74-129) is checked on short-by-long pairs."""
+    rng = np.random.default_rng(5)
+    lens = [1, 2, 600, 700, 900, 1100, 1500, 530, 3000, 4100, 2600, 5200, 800, 1700]
+    out = []
+    for i, L in enumerate(lens):
+        x = synth.step_signal(rng, L, 90.0, 12.0, 10.0, 2.0) if i % 2 else np.cumsum(rng.standard_normal(L))
+        sd = x.std()
+        out.append(((x - x.mean()) / (sd if sd else 1.0)).astype(dtype))
+    return out
+
+
+# a short centroid (629 rows after the open-end flip) against longer members
+SHORTCUT_DBA_SET = (800, 629, [4871, 4272, 660, 6390, 1776, 2009, 1535, 2535])
+
+
+def shortcut_cases(out, tmp, log):
+    """Open-end pair distances and one full-path DBA round where the
+    shortcut's partial minimum (which lane of warp 0 the check reads,
+    dtw.hpp:97-105) changes the result."""
+    for dt, sfx in ((np.float32, "f32"), (np.float64, "f64")):
+        mix = shortcut_mix_series(dt)
+        O.write_bundle(os.path.join(out, f"sc_mix_{sfx}.odbs"), mix)
+        run(["pairwise", os.path.join(out, f"sc_mix_{sfx}.odbs"),
+             os.path.join(out, f"sc_mix_{sfx}_open_end.dist.odbs"), 0, 1], log)
+        seed, Lc, lens = SHORTCUT_DBA_SET
+        STRIPE_SETS["sc"] = SHORTCUT_DBA_SET
+        centroid, members = stripe_inputs(dt, "sc")
+        del STRIPE_SETS["sc"]
+        mfile = os.path.join(out, f"sc_dba_{sfx}_members.odbs")
+        cfile = os.path.join(out, f"sc_dba_{sfx}_centroid.odbs")
+        O.write_bundle(mfile, members)
+        O.write_bundle(cfile, [centroid])
+        pfx = os.path.join(tmp, f"sc_dba_{sfx}_open_end")
+        run(["dbaupdate", mfile, cfile, pfx, 0, 1], log)
+        for ext in (".mean.odbs", ".delta.txt"):
+            if os.path.exists(pfx + ext):
+                shutil.copy(pfx + ext, os.path.join(out, f"sc_dba_{sfx}_open_end{ext}"))
+        paths_to_npz(pfx, os.path.join(out, f"sc_dba_{sfx}_open_end.paths.npz"))
+
+
 def main():
     out = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--")
                           else os.path.join(ROOT, "gpurun_out", "golden_ref"))
@@ -167,6 +316,19 @@ def main():
             chop_cases(out, tmp, log)
         shutil.rmtree(tmp, ignore_errors=True)
         print("prefix chop golden written to", out)
+        return
+    if "--stripe-only" in sys.argv:
+        with open(os.path.join(out, "harness_log_stripe.jsonl"), "w") as log:
+            stripe_cases(out, tmp, log)
+        stripe_summary(out)
+        shutil.rmtree(tmp, ignore_errors=True)
+        print("stripe golden written to", out)
+        return
+    if "--shortcut-only" in sys.argv:
+        with open(os.path.join(out, "harness_log_shortcut.jsonl"), "w") as log:
+            shortcut_cases(out, tmp, log)
+        shutil.rmtree(tmp, ignore_errors=True)
+        print("shortcut golden written to", out)
         return
     if "--clusters-only" in sys.argv:
         with open(os.path.join(out, "harness_log_clusters.jsonl"), "w") as log:
