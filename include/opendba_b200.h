@@ -240,21 +240,23 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
 /* ---- one DBA round in stripe mode ------------------------------------------------
  * Replaces DBAUpdate<T>'s stripe mode (dba.hpp:515-763), used by the
  * reference when a member's path matrix does not fit in device memory.  Same
- * arguments and results as odba_dba_round_* (bit for bit), but no member's
- * path is ever held whole: the forward pass keeps every swath's right edge
- * and every ckpt_rows-th cost row (a power of two; 0 = 4096), and the
- * backtrack recomputes, swath by swath from the right, the tiles of
+ * arguments and results as the reference's stripe mode, but no member's path
+ * is ever held whole: the forward pass keeps every swath's right edge and
+ * every ckpt_rows-th cost row (a power of two; 0 = 4096), and the backtrack
+ * recomputes, 1024-column stripe by stripe from the right, the tiles of
  * ckpt_rows rows below the path in parallel.  Workspace for the longest
- * member m and centroid length Lc: about (Lc/1024 * m + m/ckpt_rows * Lc)
- * values plus m * 256 bytes (float; double swaths are 512 wide) -- 80 GB
- * for 4 M x 4 M in float with the default, where a full path needs 4 TB.
- * Global and open-start alignment only (ODBA_ERR_INVALID_ARGUMENT with an
- * open end): there the reference's stripe mode gives its full-path results;
- * with an open end its stripe recompute applies the open-end rules at the
- * backtrack height instead of the last row, which is not reproduced. */
+ * member m and centroid length Lc (rows x columns after the open-end flip):
+ * about (Lc/1024 * m + m/ckpt_rows * Lc) values plus m * 256 bytes (float;
+ * double swaths are 512 wide) -- 80 GB for 4 M x 4 M in float with the
+ * default, where a full path needs 4 TB.  In global and open-start alignment
+ * the results equal odba_dba_round_* bit for bit.  With an open end they
+ * follow the reference's stripe re-run, which sees the backtrack height H as
+ * the first sequence's length (dba.hpp:700-721): the open-end top-row rule
+ * acts on row H-1, and the shortcut (dtw.hpp:74-129) is checked on the stored
+ * edge's rows below H, so paths and means differ from the full-path round. */
 size_t odba_dba_round_stripe_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
                                              uint64_t centroid_len, int use_open_start,
-                                             int ckpt_rows);
+                                             int use_open_end, int ckpt_rows);
 int odba_dba_round_stripe_f32(const float *centroid, uint64_t centroid_len, const float *series,
                               const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
                               int n, int use_open_start, int use_open_end, int ckpt_rows,

@@ -59,7 +59,7 @@ SIGNATURES = {
     "odba_znorm_f32": (I32, [P, P, P, I32, P, P, P]),
     "odba_znorm_f64": (I32, [P, P, P, I32, P, P, P]),
     "odba_dba_round_workspace_bytes": (ctypes.c_size_t, [I32, P, I32, U64, I32, I32]),
-    "odba_dba_round_stripe_workspace_bytes": (ctypes.c_size_t, [I32, P, I32, U64, I32, I32]),
+    "odba_dba_round_stripe_workspace_bytes": (ctypes.c_size_t, [I32, P, I32, U64, I32, I32, I32]),
     "odba_dba_round_stripe_f32": (I32, [P, U64, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P,
                                         ctypes.c_size_t, P]),
     "odba_dba_round_stripe_f64": (I32, [P, U64, P, P, P, P, I32, I32, I32, I32, P, P, P, P, P, P,

@@ -166,7 +166,7 @@ def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: in
         else:
             nbytes = lib.odba_dba_round_stripe_workspace_bytes(members.dtype.itemsize, vp(h_lens),
                                                                members.n, Lc, int(open_start),
-                                                               int(stripe_rows))
+                                                               int(open_end), int(stripe_rows))
         workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     mean = torch.empty(Lc, dtype=members.data.dtype, device=dev)
     counts = torch.empty(Lc, dtype=torch.int32, device=dev)

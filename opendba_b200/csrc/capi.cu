@@ -394,11 +394,12 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
 
 size_t odba_dba_round_stripe_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,
                                              uint64_t centroid_len, int use_open_start,
-                                             int ckpt_rows) {
+                                             int use_open_end, int ckpt_rows) {
   if (n < 1 || !h_lens || centroid_len == 0) return 0;
+  const int os = use_open_start ? 1 : 0, oe = use_open_end ? 1 : 0;
   if (elem_size == 8)
-    return dba_round_stripe_workspace_bytes<double>(h_lens, n, centroid_len, use_open_start, ckpt_rows);
-  return dba_round_stripe_workspace_bytes<float>(h_lens, n, centroid_len, use_open_start, ckpt_rows);
+    return dba_round_stripe_workspace_bytes<double>(h_lens, n, centroid_len, os, oe, ckpt_rows);
+  return dba_round_stripe_workspace_bytes<float>(h_lens, n, centroid_len, os, oe, ckpt_rows);
 }
 
 int odba_dba_round_stripe_f32(const float *centroid, uint64_t centroid_len, const float *series,

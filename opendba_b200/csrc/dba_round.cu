@@ -22,6 +22,7 @@
 // single-thread atomicAdd sequence, without atomics.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdint>
 #include <vector>
 
@@ -108,6 +109,9 @@ struct RoundArgs {
   double *deltas;
   int32_t *triples;
   int64_t *triple_counts;
+  // stripe mode with an open end: one more sample index per (member, centroid
+  // index), added after its range (-1: none)
+  const int *extra = nullptr;
 };
 
 template <typename T>
@@ -555,6 +559,13 @@ __global__ void reduce_kernel(RoundArgs<T> a) {
       const T *seq = a.series + a.offsets[a.mseries[k]];
       for (int i = r.y; i >= r.x; --i) sum = add_rn(sum, seq[i]);
       cnt += uint32_t(r.y - r.x + 1);
+      if (a.extra) {
+        const int e = a.extra[a.rng_off[k] + t];
+        if (e >= 0) {
+          sum = add_rn(sum, seq[e]);
+          ++cnt;
+        }
+      }
     }
     const T mean = cnt ? div_rn<T>(sum, T(cnt)) : host_default_nan<T>();
     a.means[a.coff[jb] + t] = mean;
@@ -821,27 +832,35 @@ int dba_batch_launch(const T *centroids, const unsigned long long *coff, const i
 
 // ---------------------------------------------------------------------------
 // Stripe mode: one DBA round for members whose 2-bit path does not fit in
-// memory (the reference's stripe mode, dba.hpp:515-763).  Per member:
+// memory (the reference's stripe mode, dba.hpp:515-763).  Per member, in the
+// orientation of the full-path round (centroid on the rows when an open end
+// flips the member, dba.hpp:497-501):
 //   1. forward: the swath pipeline (many warps, bounded hand-off waits) over
 //      the member's swaths; every swath's right edge is kept (E, one column of
 //      rows per swath) and every K-th cost row is kept across all columns (Q);
-//   2. backtrack, swath by swath from the right: every K-row tile of the swath
-//      below the current backtrack height is recomputed with its moves in
-//      parallel (one warp per tile: its row below comes from Q, its left edge
-//      from E), then one thread continues the walk through the swath and
-//      records the per-centroid-index sample ranges (and the path listing)
-//      exactly as the full-path backtrack does;
+//   2. backtrack, reference stripe by reference stripe (1024 columns) from the
+//      right: every K-row tile of the stripe's swaths below the current
+//      backtrack height H is recomputed with its moves in parallel (one warp
+//      per tile: its row below comes from Q, its left edge from E), then one
+//      warp continues the walk through the stripe and records the
+//      per-centroid-index sample ranges (and the path listing);
 //   3. the ordered reducer of the full-path round.
-// Recomputed costs equal the forward costs cell for cell, so paths, sums and
-// the delta are bit-identical to the full-path round.  Global and open-start
-// alignment only: there the reference's stripe mode gives its full-path
-// results too; with an open end its stripe recompute applies the open-end
-// rules at the backtrack height instead of the last row (dtw.hpp:74-129 with
-// first_seq_length set to the backtrack height), which is not reproduced.
+// The reference re-runs each stripe with the first sequence's length set to H
+// (dba.hpp:700-721), so with an open end its top-row rule acts on row H-1 and
+// its shortcut (dtw.hpp:74-129, open end only) is checked on the stored left
+// edge's rows below H whenever the stripe starts past column H: if it fires,
+// the stripe's row H-1 is all OPEN_RIGHT.  Stripes from the first one whose
+// shortcut fired in the forward pass on take that branch too (the reference's
+// forward pass stopped there and left those edges unwritten).  The recompute
+// here does the same: rows below H-1 are the forward pass's, row H-1 follows
+// the open-end rules (for double, whose swaths are 512 wide, the second half
+// of a stripe continues the first half's recomputed top row).  Without an open
+// end the round equals the full-path round bit for bit.
 namespace {
 
 struct StripeWalk {
   int r, c, h, cur_t, lo, hi, state;  // state: 0 walking, 1 done, 2 failed
+  int s_fwd;                          // first stripe whose forward shortcut fired, or INT_MAX
   long long nt;
 };
 
@@ -849,9 +868,10 @@ template <typename T>
 struct StripeArgs {
   const T *series;
   const uint64_t *offsets;
-  int member;                   // x = series + offsets[member]
-  const T *y;                   // centroid (columns)
-  int m, n, r0, swaths, shift;  // tile height K = 1 << shift
+  int member;                   // series + offsets[member]
+  const T *centroid;
+  int flip;                     // centroid on the rows
+  int m, n, r0, oe, swaths, shift;  // tile height K = 1 << shift
   T *E;
   unsigned long long e_stride;
   T *Q;
@@ -859,13 +879,37 @@ struct StripeArgs {
   unsigned long long *prog;     // one progress word per swath
   unsigned *err;
   unsigned long long *counter;
-  unsigned long long *words;    // one swath of moves, full-path layout
+  unsigned long long *words;    // move words of one swath, full-path layout (two buffers
+  unsigned long long words_stride;  // words_stride apart when a stripe has two swaths)
   StripeWalk *walk;
-  int2 *ranges;                 // this member's ranges (n of them)
+  int2 *ranges;                 // this member's ranges (one per centroid index)
+  int *extra;                   // this member's extra samples, or null
+  unsigned long long *fmin;     // per stripe: forward shortcut minimum (value bits)
+  unsigned long long *cmin;     // per stripe: shortcut minimum below H (value bits)
+  T *top_carry;                 // recomputed top row at the first half's right edge
   int32_t *triples;             // this member's path listing, or null
   int64_t *triple_count;        // or null
   unsigned long long limit_ns;
 };
+
+template <typename T>
+__device__ __forceinline__ const T *stripe_member_ptr(const StripeArgs<T> &a) {
+  return a.series + a.offsets[a.member];
+}
+template <typename T>
+__device__ __forceinline__ const T *stripe_rows_ptr(const StripeArgs<T> &a) {
+  return a.flip ? a.centroid : stripe_member_ptr(a);
+}
+template <typename T>
+__device__ __forceinline__ const T *stripe_cols_ptr(const StripeArgs<T> &a) {
+  return a.flip ? stripe_member_ptr(a) : a.centroid;
+}
+
+// Non-negative costs order like their bit patterns (float zero-extended).
+__device__ __forceinline__ unsigned long long cost_bits(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ unsigned long long cost_bits(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
 
 // Registers per lane of swath s (the last, partial swath is narrower).
 template <typename T>
@@ -882,19 +926,43 @@ __device__ __forceinline__ T stripe_corner(int c0, int r0) {
   return c0 == 0 ? (r0 ? Num<T>::big() : T(0)) : (r0 ? T(0) : Num<T>::big());
 }
 
+// The stored right edge of the swath ending at column c - 1 (c a multiple of
+// the swath width, 0 < c < n).
+template <typename T>
+__device__ __forceinline__ const T *stripe_edge_before(const StripeArgs<T> &a, int c) {
+  constexpr int W = 32 * PathTune<T>::RF;
+  return a.E + (unsigned long long)(c / W - 1) * a.e_stride;
+}
+
+// Whether the reference's re-run of stripe t at height H takes its shortcut
+// branch (the whole of row H-1 OPEN_RIGHT).
+template <typename T>
+__device__ __forceinline__ bool stripe_fires(const StripeArgs<T> &a, int t, int H,
+                                             const StripeWalk &w) {
+  if (!a.oe || a.r0) return false;
+  const long long L = (long long)t * kRefSwath;
+  if (L <= H) return false;
+  if (t >= w.s_fwd) return true;
+  return cost_bits(stripe_edge_before(a, int(L))[H - 1]) == a.cmin[t];
+}
+
 template <typename T, int R>
 __device__ __forceinline__ void stripe_fwd_swath(const SwathJob<T> &job, const PipeGate &gate,
                                                  const CkptOut<T> &ck) {
   T col[R];
-  sweep_swath<T, R, PipeGate, true>(job, col, gate, ck);
+  sweep_swath<T, R, PipeGate, true, false>(job, col, gate, ck);
 }
 
-template <typename T, int RF, int RQ>
+// OE: open end; FLIP: centroid on the rows (compile-time switches, so that
+// one of the two series pointers stays a kernel parameter and the sweep keeps
+// its registers)
+template <typename T, int RF, int RQ, bool OE, bool FLIP>
 __global__ void __launch_bounds__(kRoundWarps * 32) stripe_forward_kernel(StripeArgs<T> a) {
   __shared__ __align__(16) T stage_mem[kRoundWarps * kStageElems];
   constexpr int W = 32 * RF;
   const int lane = threadIdx.x & 31;
-  const T *x = a.series + a.offsets[a.member];
+  const T *x = FLIP ? a.centroid : stripe_member_ptr(a);
+  const T *y = FLIP ? stripe_member_ptr(a) : a.centroid;
   for (;;) {
     unsigned long long q = 0;
     if (lane == 0) q = atomicAdd(a.counter, 1ull);
@@ -903,14 +971,14 @@ __global__ void __launch_bounds__(kRoundWarps * 32) stripe_forward_kernel(Stripe
     const int sw = int(q), c0 = sw * W;
     SwathJob<T> job;
     job.x = x;
-    job.y = a.y;
+    job.y = y;
     job.m = a.m;
     job.n = a.n;
     job.c0 = c0;
     job.r0 = a.r0;
     job.edge_in = sw ? a.E + (unsigned long long)(sw - 1) * a.e_stride : nullptr;
     job.edge_out = sw + 1 < a.swaths ? a.E + (unsigned long long)sw * a.e_stride : nullptr;
-    job.open_end = false;
+    job.open_end = OE;
     job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
     job.corner_init = stripe_corner<T>(c0, a.r0);
     job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
@@ -945,30 +1013,86 @@ __global__ void __launch_bounds__(kRoundWarps * 32) stripe_forward_kernel(Stripe
   }
 }
 
+// Shortcut minimum of the stored edge before stripe t over rows [0, H)
+// (ShortcutRows), reduced into slot[t].  Forward pass (fwd): every stripe t
+// in [tlo, thi] (stripes past the last row), H = m.  Backtrack: the one
+// stripe tlo, H the walk's height, skipped where the stripe's branch is
+// already decided.
+template <typename T>
+__global__ void stripe_min_kernel(StripeArgs<T> a, int tlo, int thi, int fwd) {
+  __shared__ unsigned long long smin[256];
+  const StripeWalk *wp = a.walk;
+  int H = a.m;
+  if (!fwd) {
+    if (wp->state != 0) return;
+    H = wp->h;
+    if ((long long)tlo * kRefSwath <= H || tlo >= wp->s_fwd) return;
+  }
+  unsigned long long *slot = fwd ? a.fmin : a.cmin;
+  for (int t = tlo + int(blockIdx.y); t <= thi; t += int(gridDim.y)) {
+    const T *e = stripe_edge_before(a, t * kRefSwath);
+    unsigned long long best = ~0ull;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < H;
+         r += (long long)gridDim.x * blockDim.x) {
+      if (!shortcut_row<T>(int(r))) continue;
+      const unsigned long long b = cost_bits(e[r]);
+      best = b < best ? b : best;
+    }
+    smin[threadIdx.x] = best;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s && smin[threadIdx.x + s] < smin[threadIdx.x])
+        smin[threadIdx.x] = smin[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && smin[0] != ~0ull) atomicMin(slot + t, smin[0]);
+    __syncthreads();
+  }
+}
+
+// The first stripe in [tlo, thi] whose forward shortcut fires (one warp).
+template <typename T>
+__global__ void stripe_sfwd_kernel(StripeArgs<T> a, int tlo, int thi) {
+  const int lane = threadIdx.x & 31;
+  for (int t0 = tlo; t0 <= thi; t0 += 32) {
+    const int t = t0 + lane;
+    bool f = false;
+    if (t <= thi) f = cost_bits(stripe_edge_before(a, t * kRefSwath)[a.m - 1]) == a.fmin[t];
+    const unsigned ballot = __ballot_sync(kFull, f);
+    if (ballot) {
+      if (lane == 0) a.walk->s_fwd = t0 + __ffs(ballot) - 1;
+      return;
+    }
+  }
+}
+
 template <typename T, int R>
-__device__ __forceinline__ void stripe_tile_swath(const SwathJob<T> &job, const PathOut &po,
-                                                  const TileIn<T> &tile) {
+__device__ __forceinline__ T stripe_tile_swath(const SwathJob<T> &job, const PathOut &po,
+                                               const TileIn<T> &tile) {
   T col[R];
   T emin, etop;
   sweep_swath_path<T, R>(job, po, col, emin, etop, tile);
+  return etop;
 }
 
-// One warp per K-row tile of swath s below the backtrack height.
+// One warp per K-row tile of swath s below the backtrack height, into move
+// buffer buf.
 template <typename T, int RF, int RQ>
-__global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArgs<T> a, int s) {
+__global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArgs<T> a, int s, int buf) {
   __shared__ __align__(16) T stage_mem[kRoundWarps * kStageElems];
   constexpr int W = 32 * RF;
   const int kt = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
-  const int H = a.walk->h;
+  const StripeWalk w = *a.walk;
+  const int H = w.h;
   const int K = 1 << a.shift;
   const long long rb_l = (long long)a.r0 + (long long)kt * K;
-  if (a.walk->state != 0 || rb_l >= H) return;
+  const int c0 = s * W;
+  if (w.state != 0 || rb_l >= H || stripe_fires(a, c0 / kRefSwath, H, w)) return;
   const int rb = int(rb_l);
   const int re = rb + K < H ? rb + K : H;
-  const int c0 = s * W;
   SwathJob<T> job;
-  job.x = a.series + a.offsets[a.member];
-  job.y = a.y;
+  job.x = stripe_rows_ptr(a);
+  job.y = stripe_cols_ptr(a);
   job.m = re;
   job.n = a.n;
   job.c0 = c0;
@@ -976,25 +1100,28 @@ __global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArg
   const T *left = s ? a.E + (unsigned long long)(s - 1) * a.e_stride : nullptr;
   job.edge_in = left ? left + (unsigned long long)kt * K : nullptr;
   job.edge_out = nullptr;
-  job.open_end = false;
+  job.open_end = a.oe != 0;
   job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
   job.corner_init = kt == 0 ? stripe_corner<T>(c0, a.r0)
                             : (left ? left[(unsigned long long)kt * K - 1] : Num<T>::big());
   job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
   TileIn<T> tile;
   tile.col_init = kt ? a.Q + (unsigned long long)(kt - 1) * a.q_stride + c0 : nullptr;
-  tile.top_row = a.m - 1;
+  // the re-run's top row is the backtrack height's (open end), the last row otherwise
+  tile.top_row = a.oe ? H - 1 : a.m - 1;
+  tile.top_left = (a.oe && (c0 % kRefSwath) != 0) ? a.top_carry : nullptr;
   PathOut po;
-  po.words = a.words + (unsigned long long)kt * (K / 2) * 64ull;
+  po.words = a.words + (unsigned long long)buf * a.words_stride + (unsigned long long)kt * (K / 2) * 64ull;
   po.track_min = false;
   const int R = stripe_regs<T>(a.n, s);
+  T etop = T(0);
   if (R == RF) {
-    stripe_tile_swath<T, RF>(job, po, tile);
+    etop = stripe_tile_swath<T, RF>(job, po, tile);
   } else {
     switch (R / RQ) {
 #define ODBA_TCASE(K)                                                         \
   case K:                                                                     \
-    if constexpr (K * RQ < RF) stripe_tile_swath<T, K * RQ>(job, po, tile);   \
+    if constexpr (K * RQ < RF) etop = stripe_tile_swath<T, K * RQ>(job, po, tile); \
     break;
       ODBA_TCASE(1)
       ODBA_TCASE(2)
@@ -1008,6 +1135,11 @@ __global__ void __launch_bounds__(kRoundWarps * 32) stripe_tile_kernel(StripeArg
         break;
     }
   }
+  // the first half of a two-swath stripe hands its recomputed top row's last
+  // value to the second half
+  if (a.oe && re == H && (c0 % kRefSwath) == 0 && c0 + W < a.n && W < kRefSwath &&
+      (threadIdx.x & 31) == 0)
+    *a.top_carry = etop;
 }
 
 __global__ void stripe_walk_init_kernel(StripeWalk *w, int m, int n) {
@@ -1019,18 +1151,22 @@ __global__ void stripe_walk_init_kernel(StripeWalk *w, int m, int n) {
   w->lo = 1;
   w->hi = 0;
   w->state = 0;
+  w->s_fwd = INT_MAX;
   w->nt = 0;
 }
 
 // Continues the backtrack through swath s (updateCentroid's loop,
-// dba.hpp:393-421, as in backtrack_kernel) until it leaves the swath to the
-// left or reaches the start cell.  One warp: every lane holds the move word of
-// one of the 32 rows at and below the current cell (the word of the lane that
-// owns the current column), so the walk advances by shuffles and reloads the
-// window only when it leaves those 32 rows or that owner's columns.  Every
-// lane keeps the same walk state; lane 0 does the stores.
+// dba.hpp:393-421, with the stripe branch's height, dba.hpp:384-386) until it
+// leaves the swath to the left or reaches the start cell.  One warp: every
+// lane holds the move word of one of the 32 rows at and below the current
+// cell (the word of the lane that owns the current column), so the walk
+// advances by shuffles and reloads the window only when it leaves those 32
+// rows or that owner's columns.  Every lane keeps the same walk state; lane 0
+// does the stores.  The height moves to the walk's row when it leaves a
+// reference stripe (with an open end only then; a shorter re-run is the same
+// without one).
 template <typename T>
-__global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
+__global__ void stripe_walk_kernel(StripeArgs<T> a, int s, int buf) {
   const int lane = threadIdx.x & 31;
   if (blockIdx.x) return;
   StripeWalk w = *a.walk;
@@ -1039,18 +1175,29 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
   const int c0 = s * W, R = stripe_regs<T>(a.n, s);
   const int os = a.r0;
   const long long max_cells = (long long)a.m + a.n - 1;
+  const unsigned long long *words = a.words + (unsigned long long)buf * a.words_stride;
   int2 *rg = a.ranges;
   int32_t *tri = a.triples;
   const bool lead = lane == 0;
+  // rr: the member's sample index, cc: the centroid index
   auto contribute = [&](int rr, int cc) {
     if (cc != w.cur_t) {
       if (lead && w.cur_t >= 0 && w.hi >= w.lo) rg[w.cur_t] = make_int2(w.lo, w.hi);
       w.cur_t = cc;
       w.lo = rr;
       w.hi = rr;
-    } else {
+    } else if (rr == w.lo - 1) {
       w.lo = rr;
+    } else if (lead && a.extra) {
+      // past an OPEN_RIGHT run on a re-run's top row (centroid on the rows)
+      a.extra[cc] = rr;
     }
+  };
+  auto contribute_cell = [&](int r, int c) {
+    if (a.flip)
+      contribute(c, r);
+    else
+      contribute(r, c);
   };
   auto emit = [&](int mv) {
     if (lead && tri) {
@@ -1060,7 +1207,18 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
     }
     ++w.nt;
   };
-  bool swath_done = false;
+  const int H = w.h;
+  if (stripe_fires(a, c0 / kRefSwath, H, w)) {
+    // the re-run's shortcut: row H-1 of the stripe is OPEN_RIGHT throughout
+    for (; w.c >= c0; --w.c) {
+      if (w.nt >= max_cells - 1) {
+        w.state = 2;
+        break;
+      }
+      emit(kMoveOpenRight);
+    }
+  }
+  bool swath_done = w.c < c0 || w.state != 0;
   while (!swath_done && w.state == 0) {
     // window: rows w.r - lane, columns of the owner lane of w.c
     const int top = w.r, owner = (w.c - c0) / R, cbeg = c0 + owner * R;
@@ -1069,7 +1227,7 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
     if (my_row >= 1) {
       const int rr = my_row - a.r0;
       const unsigned long long t = (unsigned long long)owner + (rr >> 1);
-      word = a.words[(t * 32 + owner) * 2 + (rr & 1)];
+      word = words[(t * 32 + owner) * 2 + (rr & 1)];
     }
     for (;;) {
       int mv;
@@ -1078,6 +1236,7 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
         mv = w.c == 0 ? (os ? kMoveNilOpenRight : kMaxMoveNil) : (os ? kMoveOpenRight : kMoveRight);
       } else {
         mv = int((wv >> (2 * (w.c - cbeg))) & 3ull);
+        if (mv == kMoveRight && a.oe && w.r == H - 1) mv = kMoveOpenRight;
       }
       if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {
         // the start cell (dba.hpp:412-415)
@@ -1093,7 +1252,7 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
         break;
       }
       emit(mv);
-      if (mv != kMoveOpenRight) contribute(w.r, w.c);
+      if (mv != kMoveOpenRight) contribute_cell(w.r, w.c);
       if (mv == kMoveDiag) {
         --w.r;
         --w.c;
@@ -1107,13 +1266,13 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s) {
         break;
       }
       if (w.c < c0) {
-        w.h = w.r + 1;
         swath_done = true;
         break;
       }
       if (top - w.r >= 32 || w.c < cbeg) break;  // reload the window
     }
   }
+  if (w.state == 0 && w.c < c0 && (!a.oe || (c0 % kRefSwath) == 0)) w.h = w.r + 1;
   if (lead) {
     if (w.state == 2 && a.triple_count) *a.triple_count = -1;
     *a.walk = w;
@@ -1129,40 +1288,63 @@ int stripe_grid() {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, stripe_forward_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>, kRoundWarps * 32, 0);
+      &per_sm, stripe_forward_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, false, false>,
+      kRoundWarps * 32, 0);
   if (per_sm < 1) per_sm = 1;
   const int g = sms * per_sm;
   if (dev < 64) cached[dev] = g;
   return g;
 }
 
+// One member's matrix: rows x columns in the round's orientation.
+struct StripeDims {
+  int flip;
+  uint64_t rows, cols;
+};
+inline StripeDims stripe_dims(uint64_t len, uint64_t Lc, int oe) {
+  StripeDims d;
+  d.flip = (oe && Lc < len) ? 1 : 0;
+  d.rows = d.flip ? Lc : len;
+  d.cols = d.flip ? len : Lc;
+  return d;
+}
+
 struct StripeLayout {
   RoundLayout round;
-  size_t off_head, off_prog, off_E, off_Q, off_W, total;
-  unsigned long long e_stride, q_stride;
-  int swaths_max;
+  size_t off_head, off_prog, off_E, off_Q, off_W, off_min, off_extra, total;
+  unsigned long long e_stride, q_stride, words_stride;
+  int swaths_max, stripes_max;
 };
 
 template <typename T>
-StripeLayout stripe_layout(const uint64_t *h_lens, int n, uint64_t Lc, int os, int shift) {
+StripeLayout stripe_layout(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe, int shift) {
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   constexpr int W = 32 * PathTune<T>::RF;
-  uint64_t maxm = 1;
-  for (int k = 0; k < n; ++k) maxm = h_lens[k] > maxm ? h_lens[k] : maxm;
+  uint64_t max_rows = 1, max_cols = 1;
+  for (int k = 0; k < n; ++k) {
+    const StripeDims d = stripe_dims(h_lens[k], Lc, oe);
+    max_rows = d.rows > max_rows ? d.rows : max_rows;
+    max_cols = d.cols > max_cols ? d.cols : max_cols;
+  }
   StripeLayout S;
   S.round = round_layout<T>(n, 1, 0, (unsigned long long)n * Lc, 1);
-  S.swaths_max = int((Lc + W - 1) / W);
-  S.e_stride = (maxm + 64 + 31) / 32 * 32;
+  S.swaths_max = int((max_cols + W - 1) / W);
+  S.stripes_max = int((max_cols + kRefSwath - 1) / kRefSwath);
+  S.e_stride = (max_rows + 64 + 31) / 32 * 32;
   S.q_stride = (unsigned long long)S.swaths_max * W;
   const unsigned long long K = 1ull << shift;
-  const unsigned long long nq = (maxm - (os ? 1 : 0)) / K + 1;
-  const unsigned long long steps = (maxm + 1) / 2 + 32;
+  const unsigned long long nq = (max_rows - (os ? 1 : 0)) / K + 1;
+  const unsigned long long steps = (max_rows + 1) / 2 + 32;
+  S.words_stride = steps * 64;
+  const int bufs = (oe && W < kRefSwath) ? 2 : 1;
   size_t o = S.round.total;
   S.off_head = o; o += 256;
   S.off_prog = o; o += up(size_t(S.swaths_max) * 8);
   S.off_E = o; o += up(size_t(S.swaths_max > 1 ? S.swaths_max - 1 : 1) * S.e_stride * sizeof(T));
   S.off_Q = o; o += up(size_t(nq) * S.q_stride * sizeof(T));
-  S.off_W = o; o += up(size_t(steps) * 64 * 8);
+  S.off_W = o; o += up(size_t(bufs) * S.words_stride * 8);
+  S.off_min = o; o += up(size_t(2) * (S.stripes_max + 1) * 8);
+  S.off_extra = o; o += oe ? up(size_t(n) * Lc * 4) : 0;
   S.total = o;
   return S;
 }
@@ -1178,11 +1360,11 @@ int stripe_shift(int ckpt_rows) {
 }  // namespace
 
 template <typename T>
-size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os,
+size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe,
                                         int ckpt_rows) {
   const int sh = stripe_shift(ckpt_rows);
   if (sh < 0 || n < 1 || Lc == 0) return 0;
-  return stripe_layout<T>(h_lens, n, Lc, os, sh).total;
+  return stripe_layout<T>(h_lens, n, Lc, os, oe, sh).total;
 }
 
 template <typename T>
@@ -1191,12 +1373,9 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
                             int n, int os, int oe, int ckpt_rows, T *mean, uint32_t *counts,
                             double *delta, int32_t *triples, int64_t *triple_counts, void *ws,
                             size_t ws_bytes, cudaStream_t stream) {
-  if (oe)
-    return fail(ODBA_ERR_INVALID_ARGUMENT,
-                "stripe mode supports global and open-start alignment (an open end needs the full path)");
   const int sh = stripe_shift(ckpt_rows);
   if (sh < 0) return fail(ODBA_ERR_INVALID_ARGUMENT, "checkpoint rows must be a power of two >= 2 (0: default)");
-  const StripeLayout S = stripe_layout<T>(h_lens, n, Lc, os, sh);
+  const StripeLayout S = stripe_layout<T>(h_lens, n, Lc, os, oe, sh);
   if (ws_bytes < S.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "stripe DBA round workspace too small");
   const RoundLayout &L = S.round;
   char *base = static_cast<char *>(ws);
@@ -1205,9 +1384,10 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
       *d_mbeg = single + 2 * n + 2, *d_mend = single + 2 * n + 3;
   unsigned long long *d_coff =
       reinterpret_cast<unsigned long long *>(base + L.off_single + ((size_t(2 * n + 4) * 4 + 7) / 8) * 8);
-  const int flags = (os ? 1 : 0) | 4;
+  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
   single_job_kernel<<<(n + 255) / 256, 256, 0, stream>>>(mseries, mjob, n, d_clen, int(Lc), d_flags,
                                                         flags, d_mbeg, d_mend, d_coff);
+  int *extra = oe ? reinterpret_cast<int *>(base + S.off_extra) : nullptr;
   RoundArgs<T> a;
   a.centroids = centroid;
   a.coff = d_coff;
@@ -1228,6 +1408,7 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
   a.deltas = delta;
   a.triples = triples;
   a.triple_counts = triple_counts;
+  a.extra = extra;
   a.counter = reinterpret_cast<unsigned long long *>(base + L.off_counter);
   a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
   a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
@@ -1240,16 +1421,19 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
   const unsigned long long nr = (unsigned long long)n * Lc;
   plan_kernel<T><<<1, 32, 0, stream>>>(a);
   fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
+  if (extra) cudaMemsetAsync(extra, 0xff, size_t(nr) * 4, stream);
   if (int rc = check_launch("stripe DBA round set-up")) return rc;
 
-  constexpr int W = 32 * PathTune<T>::RF;
+  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ;
+  constexpr int W = 32 * RF;
+  constexpr int kPerStripe = kRefSwath / W;  // swaths per reference stripe
   char *head = base + S.off_head;
   StripeArgs<T> sa;
   sa.series = series;
   sa.offsets = offsets;
-  sa.y = centroid;
-  sa.n = int(Lc);
+  sa.centroid = centroid;
   sa.r0 = os ? 1 : 0;
+  sa.oe = oe ? 1 : 0;
   sa.shift = sh;
   sa.E = reinterpret_cast<T *>(base + S.off_E);
   sa.e_stride = S.e_stride;
@@ -1261,31 +1445,70 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
   sa.err = reinterpret_cast<unsigned *>(base + L.off_counter + 8);
   cudaMemsetAsync(base + L.off_counter, 0, 16, stream);
   sa.walk = reinterpret_cast<StripeWalk *>(head + 64);
+  sa.top_carry = reinterpret_cast<T *>(head + 192);
   sa.words = reinterpret_cast<unsigned long long *>(base + S.off_W);
+  sa.words_stride = S.words_stride;
+  sa.fmin = reinterpret_cast<unsigned long long *>(base + S.off_min);
+  sa.cmin = sa.fmin + (S.stripes_max + 1);
   sa.limit_ns = kWaitLimitNs;
-  const int swaths = int((Lc + W - 1) / W);
-  sa.swaths = swaths;
+  const bool check_short = oe && !os;
   const int K = 1 << sh;
   unsigned long long trip = 0;
   for (int k = 0; k < n; ++k) {
-    const int m = int(h_lens[k]);
+    const StripeDims d = stripe_dims(h_lens[k], Lc, oe);
+    const int m = int(d.rows), ncols = int(d.cols);
+    const int swaths = (ncols + W - 1) / W;
+    const int stripes = (ncols + kRefSwath - 1) / kRefSwath;
     sa.member = k;
+    sa.flip = d.flip;
     sa.m = m;
+    sa.n = ncols;
+    sa.swaths = swaths;
     sa.ranges = a.ranges + (unsigned long long)k * Lc;
+    sa.extra = extra ? extra + (unsigned long long)k * Lc : nullptr;
     sa.triples = triples ? triples + 3ull * trip : nullptr;
     sa.triple_count = triple_counts ? triple_counts + k : nullptr;
-    trip += (unsigned long long)m + Lc + 1;
+    trip += h_lens[k] + Lc + 1;
     cudaMemsetAsync(head, 0, 64, stream);
     cudaMemsetAsync(sa.prog, 0, size_t(swaths) * 8, stream);
-    stripe_walk_init_kernel<<<1, 32, 0, stream>>>(sa.walk, m, int(Lc));
+    if (check_short) cudaMemsetAsync(sa.fmin, 0xff, size_t(2) * (S.stripes_max + 1) * 8, stream);
+    stripe_walk_init_kernel<<<1, 32, 0, stream>>>(sa.walk, m, ncols);
     const int fgrid = swaths < stripe_grid<T>() * kRoundWarps ? (swaths + kRoundWarps - 1) / kRoundWarps
                                                               : stripe_grid<T>();
-    stripe_forward_kernel<T, PathTune<T>::RF, PathTune<T>::RQ><<<fgrid, kRoundWarps * 32, 0, stream>>>(sa);
+    if (!oe)
+      stripe_forward_kernel<T, RF, RQ, false, false><<<fgrid, kRoundWarps * 32, 0, stream>>>(sa);
+    else if (!d.flip)
+      stripe_forward_kernel<T, RF, RQ, true, false><<<fgrid, kRoundWarps * 32, 0, stream>>>(sa);
+    else
+      stripe_forward_kernel<T, RF, RQ, true, true><<<fgrid, kRoundWarps * 32, 0, stream>>>(sa);
+    // stripes past the last row: where the forward pass's shortcut fired first
+    const int tlo = m / kRefSwath + 1, thi = stripes - 1;
+    const int gx = (m + 2047) / 2048 < 64 ? (m + 2047) / 2048 : 64;
+    if (check_short && tlo <= thi) {
+      const int gy = thi - tlo + 1 < 1024 ? thi - tlo + 1 : 1024;
+      stripe_min_kernel<T><<<dim3(gx, gy), 256, 0, stream>>>(sa, tlo, thi, 1);
+      stripe_sfwd_kernel<T><<<1, 32, 0, stream>>>(sa, tlo, thi);
+    }
     const int tiles = (m - sa.r0 + K - 1) / K;
     const int tgrid = ((tiles > 1 ? tiles : 1) + kRoundWarps - 1) / kRoundWarps;
-    for (int sw = swaths - 1; sw >= 0; --sw) {
-      stripe_tile_kernel<T, PathTune<T>::RF, PathTune<T>::RQ><<<tgrid, kRoundWarps * 32, 0, stream>>>(sa, sw);
-      stripe_walk_kernel<T><<<1, 32, 0, stream>>>(sa, sw);
+    auto tile = [&](int s, int buf) {
+      stripe_tile_kernel<T, RF, RQ><<<tgrid, kRoundWarps * 32, 0, stream>>>(sa, s, buf);
+    };
+    auto walk = [&](int s, int buf) { stripe_walk_kernel<T><<<1, 32, 0, stream>>>(sa, s, buf); };
+    for (int t = stripes - 1; t >= 0; --t) {
+      if (check_short && t >= 1) stripe_min_kernel<T><<<dim3(gx, 1), 256, 0, stream>>>(sa, t, t, 0);
+      const int s_lo = t * kPerStripe;
+      const int s_hi = s_lo + kPerStripe - 1 < swaths - 1 ? s_lo + kPerStripe - 1 : swaths - 1;
+      if (oe && s_hi > s_lo) {
+        // the second half continues the first half's recomputed top row
+        for (int s = s_lo; s <= s_hi; ++s) tile(s, s - s_lo);
+        for (int s = s_hi; s >= s_lo; --s) walk(s, s - s_lo);
+      } else {
+        for (int s = s_hi; s >= s_lo; --s) {
+          tile(s, 0);
+          walk(s, 0);
+        }
+      }
     }
     if (int rc = check_launch("stripe DBA round member kernels")) return rc;
   }
@@ -1294,8 +1517,8 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
   return check_launch("stripe DBA round reduce");
 }
 
-template size_t dba_round_stripe_workspace_bytes<float>(const uint64_t *, int, uint64_t, int, int);
-template size_t dba_round_stripe_workspace_bytes<double>(const uint64_t *, int, uint64_t, int, int);
+template size_t dba_round_stripe_workspace_bytes<float>(const uint64_t *, int, uint64_t, int, int, int);
+template size_t dba_round_stripe_workspace_bytes<double>(const uint64_t *, int, uint64_t, int, int, int);
 template int dba_round_stripe_launch<float>(const float *, uint64_t, const float *, const uint64_t *,
                                             const uint64_t *, const uint64_t *, int, int, int, int,
                                             float *, uint32_t *, double *, int32_t *, int64_t *,

@@ -29,6 +29,27 @@ namespace odba {
 constexpr int kRefSwath = 1024;  // blockDim.x of every reference DTWDistance launch
 constexpr unsigned kFull = 0xffffffffu;
 
+// The reference's open-end shortcut (dtw.hpp:74-129) compares the swath's
+// left-edge value on the last row with a minimum that warp 0 reduces and all
+// 32 of its lanes store to one shared word (dtw.hpp:97-105); lane l's partial
+// minimum covers the rows r with r % 1024 >= 32*l.  On the B200 the float
+// build's check reads lane 0's store (all rows), the double build's lane 16's
+// (rows with r % 1024 >= 512), as its own open-end and stripe-mode runs show.
+template <typename T>
+struct ShortcutRows;
+template <>
+struct ShortcutRows<float> {
+  static constexpr int floor = 0;
+};
+template <>
+struct ShortcutRows<double> {
+  static constexpr int floor = 512;
+};
+template <typename T>
+__host__ __device__ inline bool shortcut_row(int r) {
+  return (r & (kRefSwath - 1)) >= ShortcutRows<T>::floor;
+}
+
 template <typename T>
 struct Num;
 template <>
@@ -68,8 +89,17 @@ struct SwathJob {
   T *edge_out;        // receives C[r][c_last] for r in [r0, m), or nullptr
   bool open_end;
   bool free_diag0;    // column c0 is a reference swath-left column (c0 % 1024 == 0, c0 > 0)
+  bool track = false;  // keep the right edge's shortcut minimum and last-row value (EdgeStat)
   T corner_init;      // diagonal input of lane 0 at its first row
   T *stage;           // this warp's kStageElems elements of shared memory
+};
+
+// The right-edge column's open-end shortcut figures (valid in lane 31 when the
+// job tracks them): the minimum over the rows ShortcutRows selects and the
+// value on the last row.
+template <typename T>
+struct EdgeStat {
+  T emin, etop;
 };
 
 // Staging of lane 0's row inputs: in the steady state the whole warp copies
@@ -178,10 +208,12 @@ struct CkptOut {
 
 // Sweeps one swath.  On return col[] holds, per lane, the costs of the last
 // row m-1 at the lane's columns.  Swath-edge buffers are indexed by r - r0,
-// two rows per 8/16-byte access.
-template <typename T, int R, typename Gate = NoGate, bool CKPT = false>
-__device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R], Gate gate = Gate(),
-                                            CkptOut<T> ckpt = CkptOut<T>{nullptr, 0, 1}) {
+// two rows per 8/16-byte access.  Returns the right edge's EdgeStat (lane 31;
+// the big value unless TRACK and job.track).
+template <typename T, int R, typename Gate = NoGate, bool CKPT = false, bool TRACK = true>
+__device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&col)[R],
+                                                   Gate gate = Gate(),
+                                                   CkptOut<T> ckpt = CkptOut<T>{nullptr, 0, 1}) {
   using V2 = typename Pair2<T>::V;
   const int lane = threadIdx.x & 31;
   const int m = job.m;
@@ -209,6 +241,12 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
 
   T xa_cur = T(0), xb_cur = T(0), a_last = init;
   T dg = lane0 ? job.corner_init : init;
+  const bool track = TRACK && job.track && lane31;
+  EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
+  auto note = [&](int r, T v) {
+    if (shortcut_row<T>(r)) st.emin = Num<T>::min2(st.emin, v);
+    if (r == m - 1) st.etop = v;
+  };
 
   // lane 0's inputs of step t: x of rows a, b and the left-edge costs of rows a, b
   auto fetch = [&](int t, T &xa, T &xb, T &ea, T &eb) {
@@ -253,6 +291,10 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
     if (lane31 && has_out) {
       if (act_a) job.edge_out[ra - r0] = a_last;
       if (act_b) job.edge_out[ra + 1 - r0] = col[R - 1];
+    }
+    if (track) {
+      if (act_a) note(ra, a_last);
+      if (act_b) note(ra + 1, col[R - 1]);
     }
     if (CKPT && act_b) store_ckpt(ra);
   };
@@ -348,6 +390,11 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
         *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
         if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1) gate.publish(2 * (t - 31) + 2);
       }
+      if (track) {
+        const int ra = r0 + 2 * (t - 31);
+        note(ra, a_last);
+        note(ra + 1, col[R - 1]);
+      }
     }
     // the next swath reuses the slots: no copy may still be in flight
     cp_async_wait_all();
@@ -355,6 +402,7 @@ __device__ __forceinline__ void sweep_swath(const SwathJob<T> &job, T (&col)[R],
   }
   for (; t < total; ++t) masked_step(t);
   if (Gate::kActive && lane31 && has_out) gate.publish(rows);
+  return st;
 }
 
 // Reads the cost at absolute column cabs (which must lie in this swath) from

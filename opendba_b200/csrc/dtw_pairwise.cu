@@ -66,11 +66,7 @@ __device__ __forceinline__ void pair_of(long long p, long long n, int &s_out, in
 template <typename T>
 __device__ __forceinline__ T pair_distance(T corner, int m, int n, int os, int oe) {
   float v;
-  if (m == 1 && oe && !os && n > kRefSwath) {
-    // single-row matrix: the reference's open-end shortcut reads back the
-    // sentinel it has just stored (dtw.hpp:113, 121)
-    v = __fdiv_rn(__fsqrt_rn(float(Num<T>::big())), float(m));
-  } else if ((oe && !os) || (!oe && os)) {
+  if ((oe && !os) || (!oe && os)) {
     v = __fdiv_rn(__fsqrt_rn(float(corner)), float(m));
   } else {
     v = __fsqrt_rn(float(corner));
@@ -79,10 +75,31 @@ __device__ __forceinline__ T pair_distance(T corner, int m, int n, int os, int o
 }
 
 template <typename T, int R>
-__device__ __forceinline__ void run_swath(const SwathJob<T> &job, bool last, T &corner) {
+__device__ __forceinline__ EdgeStat<T> run_swath(const SwathJob<T> &job, bool last, T &corner) {
   T col[R];
-  sweep_swath<T, R>(job, col);
+  const EdgeStat<T> st = sweep_swath<T, R>(job, col);
   if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
+  return st;
+}
+
+// The reference's open-end shortcut (dtw.hpp:74-129, open end without open
+// start) is checked on the left edge of every 1024-column reference swath that
+// starts past the last row: if that edge's value on the last row equals its
+// shortcut minimum (ShortcutRows), the swath and all later ones stop and the
+// distance is taken from that value -- from the sentinel it has just stored
+// when the matrix has one row (dtw.hpp:113, 121).  swath_checks_shortcut: the
+// swath [c0, c0 + W) whose right edge is such a left edge.
+template <typename T>
+__device__ __forceinline__ bool swath_checks_shortcut(int c0, int W, int m, int n, bool oe, int r0) {
+  const int cnext = c0 + W;
+  return oe && r0 == 0 && cnext < n && (cnext % kRefSwath) == 0 && cnext > m;
+}
+
+template <typename T>
+__device__ __forceinline__ bool shortcut_fires(const EdgeStat<T> &st, int m, T &corner) {
+  if (st.etop != st.emin) return false;
+  corner = m == 1 ? Num<T>::big() : st.etop;
+  return true;
 }
 
 // Full swaths use RF registers per lane (swath width 32*RF); the last, partial
@@ -95,6 +112,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
     const int width = job.n - c0 < W ? job.n - c0 : W;
     const bool last = c0 + W >= job.n;
     job.c0 = c0;
+    job.track = swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
     // ping-pong: swath k writes buffer k%2 and reads buffer (k+1)%2
     job.edge_in = c0 ? ((k & 1) ? e0 : e1) : nullptr;
     job.edge_out = last ? nullptr : ((k & 1) ? e1 : e0);
@@ -102,13 +120,14 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
     job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
     const int rneed = (width + 31) / 32;
     const int rq = (rneed + RQ - 1) / RQ * RQ;
+    EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
     if (rq >= RF) {
-      run_swath<T, RF>(job, last, corner);
+      st = run_swath<T, RF>(job, last, corner);
     } else {
       switch (rq / RQ) {
 #define ODBA_CASE(K)                                          \
   case K:                                                     \
-    if constexpr (K * RQ < RF) run_swath<T, K * RQ>(job, last, corner); \
+    if constexpr (K * RQ < RF) st = run_swath<T, K * RQ>(job, last, corner); \
     break;
         ODBA_CASE(1)
         ODBA_CASE(2)
@@ -124,6 +143,11 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
     }
     // the next swath's lane 0 reads what this swath's lane 31 wrote
     __syncwarp();
+    if (job.track) {
+      st.emin = __shfl_sync(kFull, st.emin, 31);
+      st.etop = __shfl_sync(kFull, st.etop, 31);
+      if (shortcut_fires<T>(st, job.m, corner)) return;
+    }
   }
 }
 
@@ -423,6 +447,8 @@ struct PipeArgs {
   unsigned long long *counter;
   unsigned *err;
   unsigned long long *progress;  // one word per (pair, swath): progress[pair * max_swaths + s]
+  T *bstat;                      // per (pair, reference swath boundary): shortcut value or -1
+  unsigned long long max_bounds;
   T *edges;                      // two buffers of edge_stride elements per pair
   unsigned long long edge_stride;
   int open_start, open_end;      // all-vs-all modes (a list carries its own)
@@ -430,11 +456,12 @@ struct PipeArgs {
 };
 
 template <typename T, int R>
-__device__ __forceinline__ void pipe_swath(const SwathJob<T> &job, const PipeGate &gate, bool last,
-                                           T &corner) {
+__device__ __forceinline__ EdgeStat<T> pipe_swath(const SwathJob<T> &job, const PipeGate &gate,
+                                                  bool last, T &corner) {
   T col[R];
-  sweep_swath<T, R, PipeGate>(job, col, gate);
+  const EdgeStat<T> st = sweep_swath<T, R, PipeGate>(job, col, gate);
   if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
+  return st;
 }
 
 template <typename T, int RF, int RQ>
@@ -485,6 +512,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     job.edge_out = last ? nullptr : ((sw & 1) ? b1 : b0);
     job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
     job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
+    job.track = swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
     PipeGate gate;
     unsigned long long *words = a.progress + qi * a.max_swaths;
     gate.prog_in = words + (sw ? sw - 1 : 0);
@@ -496,13 +524,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     const int width = job.n - c0 < W ? job.n - c0 : W;
     const int rneed = (width + 31) / 32;
     const int rq = (rneed + RQ - 1) / RQ * RQ;
+    EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
     if (rq >= RF) {
-      pipe_swath<T, RF>(job, gate, last, corner);
+      st = pipe_swath<T, RF>(job, gate, last, corner);
     } else {
       switch (rq / RQ) {
 #define ODBA_PCASE(K)                                                       \
   case K:                                                                   \
-    if constexpr (K * RQ < RF) pipe_swath<T, K * RQ>(job, gate, last, corner); \
+    if constexpr (K * RQ < RF) st = pipe_swath<T, K * RQ>(job, gate, last, corner); \
     break;
         ODBA_PCASE(1)
         ODBA_PCASE(2)
@@ -516,6 +545,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
           break;
       }
     }
+    if (job.track && lane == 31) {
+      // this swath's right edge is the left edge of reference swath k + 1
+      const unsigned long long k = (unsigned long long)(c0 + W) / kRefSwath - 1;
+      T v;
+      a.bstat[qi * a.max_bounds + k] = shortcut_fires<T>(st, job.m, v) ? v : T(-1);
+    }
     if (last && lane == 0) {
       const bool bad = *reinterpret_cast<volatile unsigned *>(a.err) != 0;
       a.dists[out] = bad ? T(NAN) : pair_distance<T>(corner, job.m, job.n, os, oe);
@@ -523,14 +558,58 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
   }
 }
 
+// After the pipeline: a pair whose open-end shortcut fired on some checked
+// edge takes its distance from the first such edge (the swaths after it ran
+// anyway; the reference's stop there).  One thread per pair.
+template <typename T>
+__global__ void pipe_shortcut_kernel(PipeArgs<T> a) {
+  const unsigned long long qi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (qi >= a.npairs) return;
+  if (*reinterpret_cast<volatile unsigned *>(a.err) != 0) return;
+  int s, j, os, oe;
+  unsigned long long out;
+  if (a.list) {
+    const odba_pair_task task = a.list[qi];
+    s = int(task.first);
+    j = int(task.second);
+    os = int((task.out >> 62) & 1ull);
+    oe = int((task.out >> 63) & 1ull);
+    out = task.out & ((1ull << 62) - 1);
+  } else {
+    const long long p = (long long)(a.pbeg + a.npairs - 1 - qi);
+    pair_of(p, a.n, s, j);
+    os = a.open_start;
+    oe = a.open_end;
+    out = (unsigned long long)p;
+  }
+  if (!oe || os) return;
+  const int m = int(a.lens[s]), n = int(a.lens[j]);
+  for (int cnext = kRefSwath; cnext < n; cnext += kRefSwath) {
+    if (cnext <= m) continue;
+    const T v = a.bstat[qi * a.max_bounds + (unsigned long long)(cnext / kRefSwath - 1)];
+    if (v >= T(0)) {
+      a.dists[out] = pair_distance<T>(v, m, n, os, oe);
+      return;
+    }
+  }
+}
+
 }  // namespace
 
-// counter and error word | progress words | edge buffers
+// counter and error word | progress words | shortcut values | edge buffers
 template <typename T>
-size_t swathpipe_head_bytes(unsigned long long npairs, uint64_t max_len) {
+size_t swathpipe_progress_bytes(unsigned long long npairs, uint64_t max_len) {
   constexpr int W = 32 * Tune<T>::RF;
   const unsigned long long max_swaths = (max_len + W - 1) / W;
-  return 256 + (size_t(npairs) * max_swaths * 8 + 255) / 256 * 256;
+  return (size_t(npairs) * max_swaths * 8 + 255) / 256 * 256;
+}
+
+inline unsigned long long swathpipe_max_bounds(uint64_t max_len) { return max_len / kRefSwath + 1; }
+
+template <typename T>
+size_t swathpipe_head_bytes(unsigned long long npairs, uint64_t max_len) {
+  return 256 + swathpipe_progress_bytes<T>(npairs, max_len) +
+         (size_t(npairs) * swathpipe_max_bounds(max_len) * sizeof(T) + 255) / 256 * 256;
 }
 
 template <typename T>
@@ -562,15 +641,20 @@ int swathpipe_launch(const T *series, const uint64_t *offsets, const uint64_t *l
   a.counter = reinterpret_cast<unsigned long long *>(base);
   a.err = reinterpret_cast<unsigned *>(base + 8);
   a.progress = reinterpret_cast<unsigned long long *>(base + 256);
+  a.bstat = reinterpret_cast<T *>(base + 256 + swathpipe_progress_bytes<T>(npairs, max_len));
+  a.max_bounds = swathpipe_max_bounds(max_len);
   const size_t head = swathpipe_head_bytes<T>(npairs, max_len);
   a.edges = reinterpret_cast<T *>(base + head);
   a.edge_stride = (max_len + 32 + 31) / 32 * 32;
   a.open_start = os;
   a.open_end = oe;
   a.limit_ns = limit_ns ? limit_ns : kWaitLimitNs;
-  if (cudaMemsetAsync(base, 0, head, stream) != cudaSuccess)
+  // the shortcut values need no clearing: every checked edge writes its entry
+  if (cudaMemsetAsync(base, 0, 256 + swathpipe_progress_bytes<T>(npairs, max_len), stream) != cudaSuccess)
     return fail(ODBA_ERR_CUDA, "clearing the pipeline state failed");
   swathpipe_kernel<T, Tune<T>::RF, Tune<T>::RQ><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
+  if (list || (oe && !os))
+    pipe_shortcut_kernel<T><<<unsigned((npairs + 127) / 128), 128, 0, stream>>>(a);
   return check_launch("swath-pipelined DTW kernel");
 }
 

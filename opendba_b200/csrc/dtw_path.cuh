@@ -106,18 +106,22 @@ struct PathOut {
 
 // A tile of a swath (stripe-mode recompute): rows [job.r0, job.m) only, the
 // row below the tile given by col_init (this lane's R columns start at
-// col_init + lane * R), and the open-end top row at top_row (the full
-// matrix's last row).  The default is a whole swath: col_init null (the
-// boundary row) and top_row = job.m - 1.
+// col_init + lane * R), and the open-end top row at top_row.  top_left, if
+// set, replaces the left-edge value of the top row (the recomputed top row of
+// the swath to the left, where that row is not the matrix's last).  The
+// default is a whole swath: col_init null (the boundary row), top_row =
+// job.m - 1, the stored left edge throughout.
 template <typename T>
 struct TileIn {
   const T *col_init;
   int top_row;
+  const T *top_left = nullptr;
 };
 
 // Sweeps one swath recording moves.  Same wavefront as sweep_swath; in
-// addition lane 31 keeps the minimum of the right-edge column it spills and
-// its top-row value (for the reference's open-end shortcut, dtw.hpp:74-129).
+// addition lane 31 keeps the minimum of the right-edge column it spills over
+// the rows ShortcutRows selects, and its top-row value (for the reference's
+// open-end shortcut, dtw.hpp:74-129).
 template <typename T, int R, typename Gate = NoGate>
 __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const PathOut &po,
                                                  T (&col)[R], T &edge_min, T &edge_top,
@@ -155,6 +159,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
 
   T xa_cur = T(0), xb_cur = T(0), a_last = init;
   T dg = lane0 ? job.corner_init : init;
+  const T top_left = (tile.top_left && lane0) ? *tile.top_left : T(0);
 
   auto fetch = [&](int t, T &xa, T &xb, T &ea, T &eb) {
     const int k = 2 * t;
@@ -167,6 +172,11 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
       if (Gate::kActive) gate.wait_in(rows > 0 ? kb + 1 : 0);
       ea = job.edge_in[ka];
       eb = job.edge_in[kb];
+      if (tile.top_left) {
+        // the top row is the tile's last, always in the masked drain
+        if (r0 + k == top) ea = top_left;
+        if (r0 + k + 1 == top) eb = top_left;
+      }
     } else {
       ea = eb = Num<T>::big();
     }
@@ -206,12 +216,12 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     if (lane31) {
       if (act_a) {
         if (has_out) job.edge_out[ra - r0] = a_last;
-        emin = Num<T>::min2(emin, a_last);
+        if (shortcut_row<T>(ra)) emin = Num<T>::min2(emin, a_last);
         if (ra == top) etop = a_last;
       }
       if (act_b) {
         if (has_out) job.edge_out[ra + 1 - r0] = col[R - 1];
-        emin = Num<T>::min2(emin, col[R - 1]);
+        if (shortcut_row<T>(ra + 1)) emin = Num<T>::min2(emin, col[R - 1]);
         if (ra + 1 == top) etop = col[R - 1];
       }
     }
@@ -311,7 +321,9 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
           if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1)
             gate.publish(2 * (t - 31) + 2);
         }
-        emin = Num<T>::min2(emin, Num<T>::min2(a_last, col[R - 1]));
+        const int ra = r0 + 2 * (t - 31);
+        if (shortcut_row<T>(ra)) emin = Num<T>::min2(emin, a_last);
+        if (shortcut_row<T>(ra + 1)) emin = Num<T>::min2(emin, col[R - 1]);
       }
     }
     // the next swath reuses the slots: no copy may still be in flight

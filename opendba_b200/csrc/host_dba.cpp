@@ -111,15 +111,13 @@ struct Ops<double> {
 
 // Full path or stripe mode for a DBA round.  Like the reference
 // (dba.hpp:515-527), stripe mode is chosen when the full-path workspace does
-// not fit in free device memory; ODBA_FORCE_STRIPE=1 forces it.  Stripe mode
-// covers global and open-start alignment; with an open end the full path is
-// always used.  Returns the workspace bytes; *stripe_rows is -1 (full path)
-// or the stripe tile height (0 = the library default).
+// not fit in free device memory; ODBA_FORCE_STRIPE=1 forces it.  Returns the
+// workspace bytes; *stripe_rows is -1 (full path) or the stripe tile height
+// (0 = the library default).
 template <typename T>
 size_t round_workspace(const uint64_t *lens, int n, uint64_t Lc, int os, int oe, int *stripe_rows) {
   const size_t full = odba_dba_round_workspace_bytes(sizeof(T), lens, n, Lc, os, oe);
   *stripe_rows = -1;
-  if (oe) return full;
   bool stripe = false;
   if (const char *f = std::getenv("ODBA_FORCE_STRIPE")) stripe = *f && *f != '0';
   if (!stripe) {
@@ -139,11 +137,11 @@ size_t round_workspace(const uint64_t *lens, int n, uint64_t Lc, int os, int oe,
     cudaGetLastError();
     rows = 1024;
     while (rows < (1 << 20) &&
-           odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, rows) > fr / 20 * 19)
+           odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, oe, rows) > fr / 20 * 19)
       rows *= 2;
   }
   *stripe_rows = rows;
-  return odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, rows);
+  return odba_dba_round_stripe_workspace_bytes(sizeof(T), lens, n, Lc, os, oe, rows);
 }
 
 // True if the launch that used workspace ws (pairwise or round) reported a

@@ -75,7 +75,7 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
                      void *ws, size_t ws_bytes, cudaStream_t stream);
 
 template <typename T>
-size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os,
+size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe,
                                         int ckpt_rows);
 template <typename T>
 int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,

@@ -252,7 +252,7 @@ def _long_round(raw):
     lib = _native.lib()
     import os
     rows = int(os.environ.get("ODBA_STRIPE_ROWS", "1024"))
-    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0, rows)
+    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0, 0, rows)
     ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()

@@ -82,6 +82,28 @@ def test_round_random_vs_oracle(env, dtype, mode):
         assert np.array_equal(paths[k], t.astype(np.int32)), f"member {k}"
 
 
+@pytest.mark.parametrize("sfx", ["f32", "f64"])
+def test_round_open_end_shortcut_lane_matches_reference_gpu(env, sfx):
+    # a 629-row centroid against longer members: the double build's shortcut
+    # reads warp-0 lane 16's partial minimum (rows r % 1024 >= 512), which
+    # changes this round's paths (the full minimum would not)
+    members = O.read_bundle(os.path.join(GOLDEN, f"sc_dba_{sfx}_members.odbs"))
+    centroid = O.read_bundle(os.path.join(GOLDEN, f"sc_dba_{sfx}_centroid.odbs"))[0]
+    ref = O.read_bundle(os.path.join(GOLDEN, f"sc_dba_{sfx}_open_end.mean.odbs"))[0]
+    with open(os.path.join(GOLDEN, f"sc_dba_{sfx}_open_end.delta.txt")) as f:
+        ref_delta = float(f.read())
+    mean, counts, delta, paths = _round(env, centroid, members, 0, 1)
+    assert np.array_equal(_bits(mean), _bits(ref))
+    assert delta == ref_delta
+    gold = np.load(os.path.join(GOLDEN, f"sc_dba_{sfx}_open_end.paths.npz"))
+    for k, seq in enumerate(members):
+        ij = gold[f"ij{k}"].copy()
+        if len(centroid) < len(seq):
+            ij[:-1] = ij[:-1, ::-1]
+        assert np.array_equal(paths[k][:, :2], ij), f"member {k} path cells"
+        assert np.array_equal(paths[k][:, 2].astype(np.uint8), gold[f"mv{k}"]), f"member {k} moves"
+
+
 def test_round_open_end_shortcut_fires(env):
     # a short member against a long flat centroid: the top row becomes the
     # column minimum early, so the reference's shortcut decides the path end

@@ -78,6 +78,32 @@ def test_every_plan_matches_reference_gpu(api, pin, plan, sfx, mode):
     assert bad.size == 0, f"{plan}: {bad.size} mismatches, first {bad[:5]}"
 
 
+@pytest.mark.parametrize("plan", list(PLANS))
+@pytest.mark.parametrize("sfx", ["f32", "f64"])
+def test_open_end_shortcut_lanes_every_plan(api, pin, plan, sfx):
+    # short-by-long open-end pairs where the reference's shortcut fires: its
+    # float build checks the full edge minimum, its double build lane 16's
+    # partial one; one-row pairs whose result the reference reads from
+    # unwritten shared memory are checked against the oracle instead
+    from test_oracle_stripe import undefined_single_row
+    series = O.read_bundle(os.path.join(GOLDEN, f"sc_mix_{sfx}.odbs"))
+    ref = O.read_bundle(os.path.join(GOLDEN, f"sc_mix_{sfx}_open_end.dist.odbs"))[0]
+    ds = api.DeviceSeries.from_host(series)
+    elem = 4 if sfx == "f32" else 8
+    npairs = len(series) * (len(series) - 1) // 2
+    pin(elem, ds.max_len, npairs, PLANS[plan])
+    ws = api.pairwise_workspace(ds)
+    assert _plan_in_use(elem, ds.max_len, npairs, ws.numel())[0] == PLANS[plan]
+    got = api.pairwise(ds, 0, 1, workspace=ws).cpu().numpy()
+    want = O.pairwise(series, 0, 1, fma_mode=1)
+    p = 0
+    for i in range(len(series) - 1):
+        for j in range(i + 1, len(series)):
+            exp = want[p] if undefined_single_row(len(series[i]), len(series[j]), sfx) else ref[p]
+            assert got[p].tobytes() == np.asarray(exp, dtype=got.dtype).tobytes(), (plan, i, j)
+            p += 1
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("mode", list(MODES))
 def test_pipeline_long_series_vs_oracle(api, pin, dtype, mode):
