@@ -74,10 +74,10 @@ __device__ __forceinline__ T pair_distance(T corner, int m, int n, int os, int o
   return T(v);
 }
 
-template <typename T, int R>
+template <typename T, int R, bool TRACK>
 __device__ __forceinline__ EdgeStat<T> run_swath(const SwathJob<T> &job, bool last, T &corner) {
   T col[R];
-  const EdgeStat<T> st = sweep_swath<T, R>(job, col);
+  const EdgeStat<T> st = sweep_swath<T, R, NoGate, false, TRACK>(job, col);
   if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
   return st;
 }
@@ -103,8 +103,10 @@ __device__ __forceinline__ bool shortcut_fires(const EdgeStat<T> &st, int m, T &
 }
 
 // Full swaths use RF registers per lane (swath width 32*RF); the last, partial
-// swath uses the smallest multiple of RQ registers that covers it.
-template <typename T, int RF, int RQ>
+// swath uses the smallest multiple of RQ registers that covers it.  TRACK:
+// the pair may take the open-end shortcut (off at compile time for launches
+// without an open end, so that their sweep carries no extra work).
+template <typename T, int RF, int RQ, bool TRACK>
 __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
   constexpr int W = 32 * RF;
   int k = 0;
@@ -112,7 +114,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
     const int width = job.n - c0 < W ? job.n - c0 : W;
     const bool last = c0 + W >= job.n;
     job.c0 = c0;
-    job.track = swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
+    job.track = TRACK && swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
     // ping-pong: swath k writes buffer k%2 and reads buffer (k+1)%2
     job.edge_in = c0 ? ((k & 1) ? e0 : e1) : nullptr;
     job.edge_out = last ? nullptr : ((k & 1) ? e1 : e0);
@@ -122,12 +124,12 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
     const int rq = (rneed + RQ - 1) / RQ * RQ;
     EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
     if (rq >= RF) {
-      st = run_swath<T, RF>(job, last, corner);
+      st = run_swath<T, RF, TRACK>(job, last, corner);
     } else {
       switch (rq / RQ) {
 #define ODBA_CASE(K)                                          \
   case K:                                                     \
-    if constexpr (K * RQ < RF) st = run_swath<T, K * RQ>(job, last, corner); \
+    if constexpr (K * RQ < RF) st = run_swath<T, K * RQ, TRACK>(job, last, corner); \
     break;
         ODBA_CASE(1)
         ODBA_CASE(2)
@@ -143,7 +145,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
     }
     // the next swath's lane 0 reads what this swath's lane 31 wrote
     __syncwarp();
-    if (job.track) {
+    if (TRACK && job.track) {
       st.emin = __shfl_sync(kFull, st.emin, 31);
       st.etop = __shfl_sync(kFull, st.etop, 31);
       if (shortcut_fires<T>(st, job.m, corner)) return;
@@ -151,7 +153,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
   }
 }
 
-template <typename T, int RF, int RQ>
+template <typename T, int RF, int RQ, bool TRACK>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     pairwise_kernel(PairwiseArgs<T> a) {
   __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     job.r0 = a.open_start ? 1 : 0;
     job.open_end = a.open_end != 0;
     T corner = T(0);
-    sweep_pair<T, RF, RQ>(job, e0, e1, corner);
+    sweep_pair<T, RF, RQ, TRACK>(job, e0, e1, corner);
     if (lane == 0) a.dists[p] = pair_distance<T>(corner, job.m, job.n, a.open_start, a.open_end);
   }
 }
@@ -201,7 +203,7 @@ int grid_size() {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ>, kWarpsPerBlock * 32, 0);
+      &per_sm, pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ, false>, kWarpsPerBlock * 32, 0);
   if (per_sm < 1) per_sm = 1;
   const int g = sms * per_sm;
   if (dev < 64) cached[dev] = g;
@@ -241,7 +243,10 @@ int whole_pairwise_launch(const T *series, const uint64_t *offsets, const uint64
   a.open_start = os;
   a.open_end = oe;
   cudaMemsetAsync(a.counter, 0, 16, stream);  // work counter and error word
-  pairwise_kernel<T, RF, Tune<T>::RQ><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
+  if (oe && !os)
+    pairwise_kernel<T, RF, Tune<T>::RQ, true><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
+  else
+    pairwise_kernel<T, RF, Tune<T>::RQ, false><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
   return check_launch("pairwise DTW kernel");
 }
 
@@ -327,7 +332,10 @@ int pairwise_noalloc(const T *series, const uint64_t *offsets, const uint64_t *l
   // the counter is the only state that must start at zero
   cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(ODBA_ERR_CUDA, "clearing the work counter failed");
-  pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ><<<grid, kWarpsPerBlock * 32, 0, stream>>>(a);
+  if (a.open_end && !a.open_start)
+    pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ, true><<<grid, kWarpsPerBlock * 32, 0, stream>>>(a);
+  else
+    pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ, false><<<grid, kWarpsPerBlock * 32, 0, stream>>>(a);
   return check_launch("pairwise DTW kernel (no-allocation variant)");
 }
 
@@ -377,7 +385,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     job.r0 = os;
     job.open_end = oe != 0;
     T corner = T(0);
-    sweep_pair<T, RF, RQ>(job, e0, e1, corner);
+    sweep_pair<T, RF, RQ, true>(job, e0, e1, corner);
     if (lane == 0) dists[out] = pair_distance<T>(corner, job.m, job.n, os, oe);
   }
 }
@@ -455,16 +463,17 @@ struct PipeArgs {
   unsigned long long limit_ns;
 };
 
-template <typename T, int R>
+template <typename T, int R, bool TRACK>
 __device__ __forceinline__ EdgeStat<T> pipe_swath(const SwathJob<T> &job, const PipeGate &gate,
                                                   bool last, T &corner) {
   T col[R];
-  const EdgeStat<T> st = sweep_swath<T, R, PipeGate>(job, col, gate);
+  const EdgeStat<T> st = sweep_swath<T, R, PipeGate, false, TRACK>(job, col, gate);
   if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
   return st;
 }
 
-template <typename T, int RF, int RQ>
+// TRACK: some pair may take the open-end shortcut (see sweep_pair)
+template <typename T, int RF, int RQ, bool TRACK>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     swathpipe_kernel(PipeArgs<T> a) {
   constexpr int W = 32 * RF;
@@ -512,7 +521,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     job.edge_out = last ? nullptr : ((sw & 1) ? b1 : b0);
     job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
     job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
-    job.track = swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
+    job.track = TRACK && swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
     PipeGate gate;
     unsigned long long *words = a.progress + qi * a.max_swaths;
     gate.prog_in = words + (sw ? sw - 1 : 0);
@@ -526,12 +535,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     const int rq = (rneed + RQ - 1) / RQ * RQ;
     EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
     if (rq >= RF) {
-      st = pipe_swath<T, RF>(job, gate, last, corner);
+      st = pipe_swath<T, RF, TRACK>(job, gate, last, corner);
     } else {
       switch (rq / RQ) {
 #define ODBA_PCASE(K)                                                       \
   case K:                                                                   \
-    if constexpr (K * RQ < RF) st = pipe_swath<T, K * RQ>(job, gate, last, corner); \
+    if constexpr (K * RQ < RF) st = pipe_swath<T, K * RQ, TRACK>(job, gate, last, corner); \
     break;
         ODBA_PCASE(1)
         ODBA_PCASE(2)
@@ -545,7 +554,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
           break;
       }
     }
-    if (job.track && lane == 31) {
+    if (TRACK && job.track && lane == 31) {
       // this swath's right edge is the left edge of reference swath k + 1
       const unsigned long long k = (unsigned long long)(c0 + W) / kRefSwath - 1;
       T v;
@@ -652,9 +661,13 @@ int swathpipe_launch(const T *series, const uint64_t *offsets, const uint64_t *l
   // the shortcut values need no clearing: every checked edge writes its entry
   if (cudaMemsetAsync(base, 0, 256 + swathpipe_progress_bytes<T>(npairs, max_len), stream) != cudaSuccess)
     return fail(ODBA_ERR_CUDA, "clearing the pipeline state failed");
-  swathpipe_kernel<T, Tune<T>::RF, Tune<T>::RQ><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
-  if (list || (oe && !os))
+  const bool track = list || (oe && !os);
+  if (track) {
+    swathpipe_kernel<T, Tune<T>::RF, Tune<T>::RQ, true><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
     pipe_shortcut_kernel<T><<<unsigned((npairs + 127) / 128), 128, 0, stream>>>(a);
+  } else {
+    swathpipe_kernel<T, Tune<T>::RF, Tune<T>::RQ, false><<<grid_size<T>(), kWarpsPerBlock * 32, 0, stream>>>(a);
+  }
   return check_launch("swath-pipelined DTW kernel");
 }
 
