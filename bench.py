@@ -220,6 +220,8 @@ def extra_results(which):
         out["long_pairs"] = workloads.run_long()
     if which == "long_round":
         out["long_pairs"] = workloads.run_long(dtypes=())
+    if which == "long_round_open_end":
+        out["long_pairs"] = workloads.run_long(dtypes=(), round_open_end=1)
     if which == "round":
         out["dba_round"] = workloads.run_round()
     if which == "long_small":
@@ -256,20 +258,23 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--n-series", type=int, default=N_SERIES,
                     help="development only: fewer series than the benchmark configuration")
-    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "long", "long_round", "long_small", "round",
+    ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "long", "long_round",
+                                                             "long_round_open_end", "long_small", "round",
                              "all"],
                     help="medoid: the metric's configuration (default); batched: many DBA jobs, "
                          "batched vs plain; serving: Poisson request stream, served vs plain; "
                          "long: 16 series of 1M-4M samples, segmentation then all-vs-all f32 and "
                          "f64 and one stripe-mode DBA round (several minutes); long_round: the "
-                         "segmentation and the DBA round only; round: one full-path DBA round of 400 "
+                         "segmentation and the DBA round only (long_round_open_end: that round with "
+                         "an open end); round: one full-path DBA round of 400 "
                          "members of 3k-8k samples; long_small: the long workload's all-vs-all "
                          "with 20k-40k samples (a profiling case); all: the medoid line with batched and serving added")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
-    if args.workload in ("batched", "serving", "long", "long_round", "long_small", "round"):
+    if args.workload in ("batched", "serving", "long", "long_round", "long_round_open_end", "long_small",
+                         "round"):
         return run_extra(args, world, rank, local)
 
     import torch

@@ -185,7 +185,7 @@ def run_serving(rate_hz, n_requests=60, seed=0x0DBA0005, budget=32 << 30, detail
 
 
 def run_long(n_series=16, len_lo=1_000_000, len_hi=4_000_000, dtypes=("f32", "f64"), minseg=4,
-             seed=0x0DBA0002 + 2, with_round=True):
+             seed=0x0DBA0002 + 2, with_round=True, round_open_end=0):
     """Few very long series: the k-segmentation DP on each raw series, then
     all-vs-all DTW (global, z-normalised) in float32 and float64, which the
     planner runs as the swath pipeline.  Device time by CUDA events."""
@@ -233,14 +233,15 @@ def run_long(n_series=16, len_lo=1_000_000, len_hi=4_000_000, dtypes=("f32", "f6
         del ds, ws, d
         torch.cuda.empty_cache()
     if with_round:
-        out["dba_round_stripe"] = _long_round(raw)
+        out["dba_round_stripe"] = _long_round(raw, round_open_end)
     return out
 
 
-def _long_round(raw):
-    """One stripe-mode DBA round (float32, global): all series aligned to the
-    middle-length one as the centroid (the full 2-bit path would need
-    ~sum(len) * len(centroid) / 4 bytes)."""
+def _long_round(raw, open_end=0):
+    """One stripe-mode DBA round (float32, global or open end): all series
+    aligned to the middle-length one as the centroid (the full 2-bit path
+    would need ~sum(len) * len(centroid) / 4 bytes); with an open end the
+    longer members are flipped (centroid on the rows)."""
     import torch
     from . import _native
     ds = api.DeviceSeries.from_host(raw)
@@ -252,18 +253,20 @@ def _long_round(raw):
     lib = _native.lib()
     import os
     rows = int(os.environ.get("ODBA_STRIPE_ROWS", "1024"))
-    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0, 0, rows)
+    nbytes = lib.odba_dba_round_stripe_workspace_bytes(4, h.ctypes.data, len(raw), len(cen), 0,
+                                                       int(open_end), rows)
     ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     a.record()
-    mean, counts, delta, _ = api.dba_round(cen, ds, 0, 0, workspace=ws, stripe_rows=rows)
+    mean, counts, delta, _ = api.dba_round(cen, ds, 0, int(open_end), workspace=ws, stripe_rows=rows)
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
     cells = float(L.sum()) * len(cen)
     full_path_tb = float(L.sum()) * len(cen) / 4 / 1e12
     return {"centroid_len": len(cen), "members": len(raw), "tile_rows": rows or 4096,
+            "mode": "open_end" if open_end else "global",
             "seconds": ms / 1e3,
             "forward_cells": cells, "gcups": cells / ms / 1e6, "workspace_gb": nbytes / 1e9,
             "full_path_would_need_tb": full_path_tb, "delta": float(delta),
