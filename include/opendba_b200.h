@@ -56,7 +56,12 @@ int odba_device_check(void);
  * by default for n series (few long series: per-pair edge buffers instead of
  * per-warp ones).  A smaller workspace restricts the plans to those that fit.
  * use_open_start / use_open_end have the reference's meaning
- * (openDBA.cu:72-104).  If a swath hand-off wait of the pipelined plan runs
+ * (openDBA.cu:72-104), including its open-end shortcut (dtw.hpp:74-129):
+ * where it fires the distance is the last-row value of that swath's left
+ * edge.  The shortcut compares that value with a minimum the reference's float
+ * build takes over the whole edge and its double build over the edge rows r
+ * with r % 1024 >= 512 (which of its warp-0 lanes' shared stores survives, as
+ * its B200 runs show); both are reproduced.  If a swath hand-off wait of the pipelined plan runs
  * out (it never does in a healthy launch), the pairs it touched read NaN and
  * the word at byte 8 of the workspace is non-zero. */
 size_t odba_dtw_pairwise_workspace_bytes(int elem_size, uint64_t max_len);
