@@ -75,3 +75,29 @@ def test_tuning_table_set_save_load_without_gpu(native, tmp_path):
     assert lib.odba_tune_load(str(bad).encode()) == 7
     lib.odba_tune_set(4, 21, 6, 0)
     lib.odba_tune_set(8, 12, 20, 0)
+
+
+def test_stripe_workspace_sizes_without_gpu(native):
+    # host-only size queries of the stripe-mode round: an open end adds the
+    # per-(member, centroid index) extra samples and, for double (512-column
+    # swaths), a second move buffer; members longer than the centroid are
+    # flipped, so their rows are the centroid's
+    f = native.odba_dba_round_stripe_workspace_bytes
+    f.restype = ctypes.c_size_t
+    f.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                  ctypes.c_int, ctypes.c_int]
+    short = (ctypes.c_uint64 * 3)(5000, 11000, 9000)  # all shorter than the centroid
+    for elem in (4, 8):
+        g = f(elem, short, 3, 12000, 0, 0, 1024)
+        o = f(elem, short, 3, 12000, 0, 1, 1024)
+        assert g > 0 and o > g
+        assert f(elem, short, 3, 12000, 0, 0, 48) == 0  # not a power of two
+        assert f(elem, short, 3, 12000, 0, 0, 0) == f(elem, short, 3, 12000, 0, 0, 4096)
+    # double's second move buffer: one swath of moves for the longest row count
+    extra_f = f(4, short, 3, 12000, 0, 1, 1024) - f(4, short, 3, 12000, 0, 0, 1024)
+    extra_d = f(8, short, 3, 12000, 0, 1, 1024) - f(8, short, 3, 12000, 0, 0, 1024)
+    assert extra_d > extra_f
+    # a member longer than the centroid: with an open end its rows are the
+    # centroid's 12000 instead of its own 40000, so the move buffer shrinks
+    long = (ctypes.c_uint64 * 2)(5000, 40000)
+    assert f(4, long, 2, 12000, 0, 1, 1024) < f(4, long, 2, 12000, 0, 0, 1024)
