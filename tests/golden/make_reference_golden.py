@@ -2,13 +2,13 @@
 
 Test infrastructure.  Runs oracle/_ref/ref_harness (the reference's sources
 compiled for sm_100a by oracle/Makefile) on seeded inputs and stores its
-outputs under an output directory (default gpurun_out/golden_ref).  The
+outputs under the given output directory (inside the repository).  The
 committed copy lives in tests/golden/ref/; tests compare the CUDA path and
 the CPU oracle against it.
 
 Run on a B200 box from the repository root:
-    python tests/golden/make_reference_golden.py [out_dir] [--clusters-only | --chop-only |
-                                                           --stripe-only | --shortcut-only]
+    python tests/golden/make_reference_golden.py out_dir [--clusters-only | --chop-only |
+                                                          --stripe-only | --shortcut-only]
 """
 from __future__ import annotations
 
@@ -306,8 +306,10 @@ def shortcut_cases(out, tmp, log):
 
 
 def main():
-    out = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--")
-                          else os.path.join(ROOT, "gpurun_out", "golden_ref"))
+    if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
+        sys.exit("usage: make_reference_golden.py out_dir [--clusters-only | --chop-only | "
+                 "--stripe-only | --shortcut-only | --timing]")
+    out = os.path.abspath(sys.argv[1])
     os.makedirs(out, exist_ok=True)
     tmp = os.path.join(out, "_tmp")
     os.makedirs(tmp, exist_ok=True)
@@ -416,7 +418,9 @@ def main():
         "gld": (0, 0, ["random_large0.txt", "random_large1.txt"]),
     }
     for name, (os_, oe, files) in sections.items():
-        pfx = os.path.join("gpurun_out", "golden_ref", "_tmp", f"sar_{name}")
+        # a prefix relative to the repository root: the reference names its
+        # outputs after the prefix up to its first '.'
+        pfx = os.path.relpath(os.path.join(tmp, f"sar_{name}"), ROOT)
         args = ["setupandrun", pfx, os_, oe, 0] + [f"{FIXTURES}/{f}" for f in files]
         run(args, log, cwd=ROOT)
         for ext in (".avg.txt", ".pair_dists.txt"):
@@ -449,9 +453,9 @@ def main():
     if "--timing" in sys.argv:
         c2 = synth.znorm_host(synth.nanopore_like(2000, 2000, 8000, synth.SEED_BASE + 2))
         c2 = sorted(c2, key=len)
-        tpath = os.path.join(ROOT, "gpurun_out", "c2_input.odbs")
+        tpath = os.path.join(out, "c2_input.odbs")
         O.write_bundle(tpath, c2)
-        p = run(["pairwise", tpath, os.path.join(ROOT, "gpurun_out", "c2_ref_rows.dist.odbs"), 0, 0, 40], log)
+        p = run(["pairwise", tpath, os.path.join(out, "c2_ref_rows.dist.odbs"), 0, 0, 40], log)
         print("reference timing:", p.stdout.strip())
         os.remove(tpath)
     log.close()
