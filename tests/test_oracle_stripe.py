@@ -143,3 +143,25 @@ def test_open_end_full_path_round_shortcut_lanes(sfx):
         finally:
             O.set_shortcut_lanes()
         assert not np.array_equal(other.view(np.uint8), want.view(np.uint8))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_oracle_stripe_round_properties(dtype):
+    # size-independent properties of the restatement on random ragged inputs:
+    # global and open start equal the full-path round; with an open end a
+    # centroid of one stripe (1024 columns or fewer) leaves the re-run's
+    # height at the last row, so the full-path round again
+    rng = np.random.default_rng(2024)
+    for Lc in (1, 7, 1000, 1024, 1025, 2500):
+        centroid = (np.cumsum(rng.standard_normal(Lc)) * 0.1).astype(dtype)
+        for os_, oe in ((0, 0), (1, 0), (0, 1), (1, 1)):
+            if oe and Lc > 1024:
+                continue
+            # with an open end keep every member within one stripe either way
+            hi = 1025 if oe else 2600
+            members = [(np.cumsum(rng.standard_normal(int(L))) * 0.1).astype(dtype)
+                       for L in rng.integers(1, hi, size=5)]
+            st = O.dba_update_stripe(centroid, members, os_, oe)
+            full = O.dba_update(centroid, members, os_, oe)
+            assert np.array_equal(st[0].view(np.uint8), full[0].view(np.uint8)), (Lc, os_, oe)
+            assert np.array_equal(st[1], full[1]), (Lc, os_, oe)
