@@ -252,21 +252,21 @@ bool write_path_file(const std::string &fname, const char *name, const std::vect
     std::cerr << "Cannot write to " << fname << std::endl;
     return false;
   }
-  path << name << std::endl;
+  // the reference's bytes (io_utils.hpp:287-323 ends lines with std::endl);
+  // '\n' without the per-line flush keeps them in the stream's buffer
+  path << name << '\n';
   for (int64_t k = 0; k + 1 < count; ++k) {
     const int i = tri[3 * k], j = tri[3 * k + 1], mv = tri[3 * k + 2];
     if (flip)
-      path << j << "\t" << seq[j] << "\t" << i << "\t" << centroid[i] << "\t" << move_name(mv)
-           << std::endl;
+      path << j << '\t' << seq[j] << '\t' << i << '\t' << centroid[i] << '\t' << move_name(mv) << '\n';
     else
-      path << i << "\t" << seq[i] << "\t" << j << "\t" << centroid[j] << "\t" << move_name(mv)
-           << std::endl;
+      path << i << '\t' << seq[i] << '\t' << j << '\t' << centroid[j] << '\t' << move_name(mv) << '\n';
   }
   if (count > 0) {
     const int64_t k = count - 1;
     const int i = tri[3 * k], j = tri[3 * k + 1], mv = tri[3 * k + 2];
-    path << i << "\t" << seq[i] << "\t" << j << "\t" << centroid[j] << "\t"
-         << (mv == 255 ? "NIL" : (mv == 5 ? "NIL_OPEN_RIGHT" : "?")) << std::endl;
+    path << i << '\t' << seq[i] << '\t' << j << '\t' << centroid[j] << '\t'
+         << (mv == 255 ? "NIL" : (mv == 5 ? "NIL_OPEN_RIGHT" : "?")) << '\n';
   }
   return true;
 }
