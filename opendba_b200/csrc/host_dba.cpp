@@ -31,6 +31,7 @@
 
 #include "opendba.hpp"
 #include "opendba_b200.h"
+#include "text_parse.h"
 
 namespace {
 
@@ -870,37 +871,36 @@ void adaptive_segmentation(T **sequences, size_t *seq_lengths, int num_seqs, int
 
 namespace {
 
+// One value per line for every newline in the file (a last line without one
+// is not read), each the first token of its line (parse_line_value).
 template <typename T>
 int read_text_data(const char *fname, std::vector<T> &out) {
-  std::ifstream ifs(fname);
+  std::ifstream ifs(fname, std::ios::binary);
   if (!ifs) {
     std::cerr << "Error reading in file " << fname << ", skipping" << std::endl;
     return 1;
   }
-  size_t lines = 0;
+  std::string text;
   {
     std::vector<char> buf(1 << 20);
     while (true) {
       ifs.read(buf.data(), buf.size());
       const std::streamsize got = ifs.gcount();
       if (got <= 0) break;
-      lines += size_t(std::count(buf.begin(), buf.begin() + got, '\n'));
+      text.append(buf.data(), size_t(got));
     }
   }
+  const size_t lines = size_t(std::count(text.begin(), text.end(), '\n'));
   if (lines == 0) {
     std::cerr << "File " << fname << " is empty or not properly formatted. Skipping." << std::endl;
     return 1;
   }
   out.assign(lines, T(0));
-  ifs.clear();
-  ifs.seekg(0, std::ios::beg);
-  std::stringstream in;
-  std::string line;
+  const char *p = text.data();
   for (size_t i = 0; i < lines; ++i) {
-    std::getline(ifs, line);
-    in.str(line);
-    in >> out[i];
-    in.clear();
+    const char *nl = static_cast<const char *>(std::memchr(p, '\n', text.data() + text.size() - p));
+    out[i] = odba::parse_line_value<T>(p, nl);
+    p = nl + 1;
   }
   return 0;
 }
