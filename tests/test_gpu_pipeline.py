@@ -152,6 +152,38 @@ def test_cli_text_inputs(built, tmp_path):
     assert _read(prefix + ".avg.txt") == want
 
 
+@pytest.mark.parametrize("kind", ["tsv", "binary"])
+@pytest.mark.parametrize("ty", ["float", "double"])
+def test_cli_tsv_and_binary_inputs(built, tmp_path, kind, ty):
+    # the other two read modes of the CLI (cpu_utils.hpp:60-91, 381-456): one
+    # TSV file with a named series per line, or one raw binary file per series
+    dt = np.float32 if ty == "float" else np.float64
+    fmt = "%.9g" if ty == "float" else "%.17g"  # both parse back exactly
+    rng = np.random.default_rng(9 if kind == "tsv" else 10)
+    series = [(np.cumsum(rng.standard_normal(int(rng.integers(50, 400)))) + 20).astype(dt)
+              for _ in range(5)]
+    if kind == "tsv":
+        fn = tmp_path / "in.tsv"
+        fn.write_text("".join(f"s{k}" + "".join("\t" + fmt % v for v in x) + "\n"
+                              for k, x in enumerate(series)))
+        files, names = [str(fn)], [f"s{k}" for k in range(len(series))]
+    else:
+        files = []
+        for k, x in enumerate(series):
+            fn = tmp_path / f"in{k}.bin"
+            x.tofile(fn)
+            files.append(str(fn))
+        names = [f.split(".")[0] for f in files]
+    prefix = str(tmp_path / f"cli_{kind}_{ty}")
+    cli = os.path.join(ROOT, "opendba_b200", "bin", "openDBA")
+    p = subprocess.run([cli, kind, ty, "global", prefix, "0", "/dev/null", "1"] + files,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    r = O.perform_dba(series, 0, 0, norm=1, fma_mode=1)
+    want = names[r["order"][r["medoid"]]] + "".join("\t" + "%g" % float(v) for v in r["centroid"]) + "\n"
+    assert _read(prefix + ".avg.txt") == want
+
+
 def test_cli_rejects_bad_arguments(built, tmp_path):
     cli = os.path.join(ROOT, "opendba_b200", "bin", "openDBA")
     p = subprocess.run([cli, "text", "float"], capture_output=True, text=True)
