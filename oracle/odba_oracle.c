@@ -513,6 +513,73 @@ DEFINE_ZNORM(double, f64)
 DEFINE_FAST(float, f32, fmaf, fminf, FLT_MAX)
 DEFINE_FAST(double, f64, fma, fmin, DBL_MAX)
 
+/* FP64 reference distances: the recurrence, tie order, swath rules and
+ * open-end shortcut of the reference (dtw.hpp:74-239) evaluated in double
+ * whatever the result type, with the epilogue's square root and division in
+ * double too (the reference takes sqrtf even for double, dtw.hpp:116-125,
+ * 242-257).  Not a parity target: it states how far the float and double
+ * results are from FP64 arithmetic.  for_f32 picks the shortcut lane and the
+ * one-row sentinel of the float build, else those of the double build. */
+int oracle_pairwise_fp64ref(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                            int n, int os, int oe, int for_f32, double *out,
+                            const int64_t *pair_list, int64_t n_list, int threads) {
+  int64_t npairs = (int64_t)n * (n - 1) / 2;
+  int64_t count = pair_list ? n_list : npairs;
+  int64_t *row_of = (int64_t *)malloc(sizeof(int64_t) * (npairs > 0 ? npairs : 1));
+  int64_t *col_of = (int64_t *)malloc(sizeof(int64_t) * (npairs > 0 ? npairs : 1));
+  int64_t p = 0;
+  uint64_t maxlen = 1;
+  for (int s = 0; s < n; ++s)
+    if (lens[s] > maxlen) maxlen = lens[s];
+  for (int s = 0; s + 1 < n; ++s)
+    for (int j = s + 1; j < n; ++j) {
+      row_of[p] = s;
+      col_of[p] = j;
+      ++p;
+    }
+  const int saved_lane = g_shortcut_lane[1];
+  g_shortcut_lane[1] = for_f32 ? g_shortcut_lane[0] : saved_lane; /* read by sweep_f64 */
+  const double sentinel = for_f32 ? (double)FLT_MAX : DBL_MAX;
+  const int shortcut = oe && !os;
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel
+  {
+    double *a = (double *)malloc(sizeof(double) * maxlen);
+    double *b = (double *)malloc(sizeof(double) * maxlen);
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t q = 0; q < count; ++q) {
+      int64_t idx = pair_list ? pair_list[q] : q;
+      int64_t s = row_of[idx], j = col_of[idx];
+      const double *x = series + offsets[s], *y = series + offsets[j];
+      size_t m = lens[s], nn = lens[j];
+      double value;
+      if (shortcut) {
+        size_t nb = nn / SWATH + 1;
+        double *bmin = (double *)malloc(sizeof(double) * nb);
+        double *btop = (double *)calloc(nb, sizeof(double));
+        double last = sweep_f64(x, m, y, nn, os, oe, 1, NULL, bmin, btop, NULL);
+        size_t c0 = shortcut_col_f64(m, nn, os, oe, bmin, btop);
+        if (c0 && m == 1)
+          value = sqrt(sentinel) / (double)m;
+        else
+          value = sqrt(c0 ? btop[c0 / SWATH] : last) / (double)m;
+        free(bmin);
+        free(btop);
+      } else {
+        double corner = fast_pair_f64(x, m, y, nn, os, oe, a, b);
+        value = os && !oe ? sqrt(corner) / (double)m : sqrt(corner);
+      }
+      out[idx] = value;
+    }
+    free(a);
+    free(b);
+  }
+  g_shortcut_lane[1] = saved_lane;
+  free(row_of);
+  free(col_of);
+  return 0;
+}
+
 /* ---- k-segmentation (segmentation.hpp:48-337 kernel, 340-583 host) ---------
  * One "block" = raw_samples_per_threadblock = 256 * dw samples of one series,
  * processed as the reference's 256-thread block does, thread by thread.

@@ -64,6 +64,14 @@ int oracle_pairwise_fast_f64(const double *series, const uint64_t *offsets, cons
                              int n, int open_start, int open_end, double *out,
                              const int64_t *pair_list, int64_t n_list, int threads);
 
+/* FP64 reference distances for stating the error of a result: the same
+ * recurrence, tie order, swath rules and open-end shortcut evaluated in double
+ * (series given as double), square root and division in double.  for_f32
+ * selects the float build's shortcut lane and one-row sentinel. */
+int oracle_pairwise_fp64ref(const double *series, const uint64_t *offsets, const uint64_t *lens,
+                            int n, int open_start, int open_end, int for_f32, double *out,
+                            const int64_t *pair_list, int64_t n_list, int threads);
+
 /* Medoid selection of approximateMedoidIndices for one cluster (dba.hpp:186-351):
  * sums of squared distances accumulated in T in row-major pair order. */
 int oracle_medoid_f32(const float *dists, int n, const uint64_t *lens, float *sos_out);
