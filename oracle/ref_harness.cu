@@ -121,13 +121,24 @@ static int run_pairwise(const SeriesBundle &b, const std::string &out, int os, i
   double cells = 0;
   for (size_t s = 0; s < rows; ++s)
     for (size_t j = s + 1; j < n; ++j) cells += double(b.lens[s]) * double(b.lens[j]);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  // Timed by the host clock between two device synchronisations: the launches
+  // go to non-blocking streams, which an event on the legacy stream does not
+  // wait for.  Boundary buffers are released every kDrainRows rows (the
+  // reference frees them in stream callbacks, dba.hpp:157-160) so the whole
+  // triangle of a large set never holds them all at once.
+  constexpr size_t kDrainRows = 256;
   cudaDeviceSynchronize();
-  cudaEventRecord(e0, 0);
+  const auto t0 = std::chrono::steady_clock::now();
   std::vector<T *> bufs;
   std::vector<cudaStream_t> streams;
+  auto drain = [&]() {
+    cudaDeviceSynchronize();
+    CUERR("harness: pairwise sync");
+    for (auto p : bufs) cudaFree(p);
+    for (auto st : streams) cudaStreamDestroy(st);
+    bufs.clear();
+    streams.clear();
+  };
   for (size_t s = 0; s < rows; ++s) {
     dim3 grid(n - s - 1, 1, 1);
     size_t bytes = sizeof(T) * lens[s] * grid.x;
@@ -147,14 +158,11 @@ static int run_pairwise(const SeriesBundle &b, const std::string &out, int os, i
     bufs.push_back(cost);
     bufs.push_back(newcost);
     streams.push_back(st);
+    if ((s + 1) % kDrainRows == 0) drain();
   }
-  cudaEventRecord(e1, 0);
-  cudaDeviceSynchronize();
-  CUERR("harness: pairwise sync");
-  float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
-  for (auto p : bufs) cudaFree(p);
-  for (auto st : streams) cudaStreamDestroy(st);
+  drain();
+  const double ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   std::vector<T> host(npairs);
   cudaMemcpy(host.data(), dists, sizeof(T) * npairs, cudaMemcpyDeviceToHost);
   CUERR("harness: distance copy");

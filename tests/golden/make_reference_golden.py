@@ -8,7 +8,8 @@ the CPU oracle against it.
 
 Run on a B200 box from the repository root:
     python tests/golden/make_reference_golden.py out_dir [--clusters-only | --chop-only |
-                                                          --stripe-only | --shortcut-only]
+                                                          --stripe-only | --shortcut-only |
+                                                          --configs-only]
 """
 from __future__ import annotations
 
@@ -33,11 +34,25 @@ MODES = {"global": (0, 0), "open_start": (1, 0), "open_end": (0, 1), "open": (1,
 FIXTURES = "tests/golden/ref_fixtures"
 
 
+OUT = None  # the output directory, written "<out>" in the logs
+
+
+def _logged(a) -> str:
+    """An argument as the log records it: paths under the output directory as
+    <out>/..., other paths under the repository relative to its root."""
+    a = str(a)
+    if OUT and a.startswith(OUT + os.sep):
+        return "<out>/" + os.path.relpath(a, OUT)
+    if a.startswith(ROOT + os.sep):
+        return os.path.relpath(a, ROOT)
+    return a
+
+
 def run(args, log, cwd=None, env=None):
     t0 = time.time()
     p = subprocess.run([HARNESS] + [str(a) for a in args], capture_output=True, text=True, cwd=cwd,
                        env=env)
-    log.write(json.dumps({"args": [str(a) for a in args], "rc": p.returncode,
+    log.write(json.dumps({"args": [_logged(a) for a in args], "rc": p.returncode,
                           "secs": round(time.time() - t0, 3), "stdout": p.stdout[-2000:],
                           "stderr": p.stderr[-2000:]}) + "\n")
     log.flush()
@@ -134,7 +149,7 @@ def chop_cases(out, tmp, log):
         p = subprocess.run([HARNESS, "setupandrun", pfx, "0", "0", str(norm)] +
                            [os.path.basename(x) for x in paths],
                            capture_output=True, text=True, env=env, cwd=d)
-        log.write(json.dumps({"args": ["setupandrun", pfx, 0, 0, norm], "rc": p.returncode,
+        log.write(json.dumps({"args": ["setupandrun", _logged(pfx), 0, 0, norm], "rc": p.returncode,
                               "secs": round(time.time() - t0, 3), "stderr": p.stderr[-2000:]}) + "\n")
         for ext in (".prefix_chop.txt", ".avg.txt", ".pair_dists.txt"):
             if os.path.exists(pfx + ext):
@@ -201,6 +216,75 @@ def stripe_safe(centroid, members, os_, oe):
 def _sha(b: bytes) -> str:
     import hashlib
     return hashlib.sha256(b).hexdigest()
+
+
+# Every C2_SAMPLE_STRIDE-th pair distance of the medoid configuration is kept
+# verbatim (bit patterns) beside the digest of all of them.
+C2_SAMPLE_STRIDE = 997
+
+
+def c2_inputs():
+    """The medoid benchmark configuration: 2000 step signals of U[2000, 8000]
+    samples (synth.medoid_workload, seed 0x0DBA0002), z-normalised by the
+    oracle's restatement of normalizeSequences (float32)."""
+    raw = synth.medoid_workload(2000, 2000, 8000, synth.SEED_BASE + 2)
+    normed, _, _ = O.znorm(raw)
+    return normed
+
+
+def c2_cases(out, tmp, log):
+    """The reference on the medoid benchmark configuration itself (global,
+    float32): the full distance triangle from the launch loop of
+    approximateMedoidIndices (pairwise mode), then approximateMedoidIndices
+    (medoid and pair_dists.txt).  Kept as digests, the medoid, a strided
+    sample of distances and the timing in c2_medoid_ref.json."""
+    series = c2_inputs()
+    inp = os.path.join(tmp, "c2_input.odbs")
+    O.write_bundle(inp, series)
+    dist_path = os.path.join(tmp, "c2.dist.odbs")
+    p = run(["pairwise", inp, dist_path, 0, 0], log)
+    timing = json.loads(p.stdout.strip().splitlines()[-1])
+    d = O.read_bundle(dist_path)[0]
+    pfx = os.path.join(tmp, "c2_medoid")
+    t0 = time.time()
+    run(["medoid", inp, pfx, 0, 0], log)
+    medoid_secs = time.time() - t0
+    with open(pfx + ".medoid.txt") as f:
+        medoid_ref = int(f.read().split()[0])
+    with open(pfx + ".pair_dists.txt", "rb") as f:
+        txt_sha = _sha(f.read())
+    lens = np.array([len(s) for s in series], dtype=np.uint64)
+    med_from_dists, _ = O.medoid(d, lens)
+    idx = np.arange(0, len(d), C2_SAMPLE_STRIDE, dtype=np.int64)
+    rec = {"config": "2000 series, lengths U[2000,8000], global, float32",
+           "input": "synth.medoid_workload(2000, 2000, 8000, 0x0DBA0002) z-normalised by oracle.znorm",
+           "input_sha256": _sha(np.concatenate(series).tobytes()),
+           "lens_sha256": _sha(lens.tobytes()),
+           "pairs": int(len(d)), "dist_sha256": _sha(np.ascontiguousarray(d, np.float32).tobytes()),
+           "medoid": medoid_ref, "medoid_from_dists": int(med_from_dists),
+           "pair_dists_txt_sha256": txt_sha,
+           "sample_stride": C2_SAMPLE_STRIDE,
+           "sample_bits": [int(v) for v in d[idx].view(np.uint32)],
+           "reference_timing": timing, "reference_medoid_pass_secs": round(medoid_secs, 1)}
+    with open(os.path.join(out, "c2_medoid_ref.json"), "w") as f:
+        json.dump(rec, f)
+        f.write("\n")
+
+
+def c1_perform_cases(out, tmp, log):
+    """performDBA on the plain-DBA configuration (64 Gaussian random walks of
+    U[512, 1024] samples, seed 0x0DBA0001, raw values, z-normalisation on,
+    global, float32) until it converges: avg.txt, pair_dists.txt and the last
+    round's path of every member."""
+    ser = synth.random_walks(64, 512, 1024, synth.SEED_BASE + 1)
+    src = os.path.join(out, "perform_c1_f32.odbs")
+    O.write_bundle(src, ser)
+    pfx = os.path.join(tmp, "perform_c1_f32_global")
+    run(["performdba", src, pfx, 0, 0, 1], log)
+    for ext in (".avg.txt", ".pair_dists.txt"):
+        if os.path.exists(pfx + ext):
+            shutil.copy(pfx + ext, os.path.join(out, f"perform_c1_f32_global{ext}"))
+    paths_to_npz(pfx + ".0", os.path.join(out, "perform_c1_f32_global.paths.npz"))
 
 
 def path_digest(ij: np.ndarray, mv: np.ndarray) -> str:
@@ -308,8 +392,10 @@ def shortcut_cases(out, tmp, log):
 def main():
     if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
         sys.exit("usage: make_reference_golden.py out_dir [--clusters-only | --chop-only | "
-                 "--stripe-only | --shortcut-only | --timing]")
+                 "--stripe-only | --shortcut-only | --configs-only | --timing]")
+    global OUT
     out = os.path.abspath(sys.argv[1])
+    OUT = out
     os.makedirs(out, exist_ok=True)
     tmp = os.path.join(out, "_tmp")
     os.makedirs(tmp, exist_ok=True)
@@ -331,6 +417,13 @@ def main():
             shortcut_cases(out, tmp, log)
         shutil.rmtree(tmp, ignore_errors=True)
         print("shortcut golden written to", out)
+        return
+    if "--configs-only" in sys.argv:
+        with open(os.path.join(out, "harness_log_configs.jsonl"), "w") as log:
+            c1_perform_cases(out, tmp, log)
+            c2_cases(out, tmp, log)
+        shutil.rmtree(tmp, ignore_errors=True)
+        print("benchmark-configuration golden written to", out)
         return
     if "--clusters-only" in sys.argv:
         with open(os.path.join(out, "harness_log_clusters.jsonl"), "w") as log:
