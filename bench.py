@@ -49,19 +49,7 @@ SM_MAX_MHZ = 1965.0
 
 def workload(rank: int, n_series: int = N_SERIES):
     from opendba_b200 import synth
-    rng = np.random.default_rng(SEED + rank)
-    lens = rng.integers(LEN_LO, LEN_HI + 1, size=n_series)
-    series = []
-    for L in lens:
-        # vectorised step signal: geometric dwells, N(90,12) levels, N(0,2) noise
-        dw = rng.geometric(0.1, size=int(L) // 4 + 16)
-        while dw.sum() < L:
-            dw = np.concatenate([dw, rng.geometric(0.1, size=int(L) // 4 + 16)])
-        levels = rng.normal(90.0, 12.0, size=len(dw))
-        x = np.repeat(levels, dw)[:L] + rng.normal(0.0, 2.0, size=int(L))
-        series.append(x.astype(np.float32))
-    series.sort(key=len)  # performDBA sorts by length before the medoid pass (dba.hpp:876-885)
-    return series, synth
+    return synth.medoid_workload(n_series, LEN_LO, LEN_HI, SEED + rank), synth
 
 
 def cells_of(lens) -> float:

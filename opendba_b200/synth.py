@@ -52,6 +52,27 @@ def nanopore_like(n: int, lo: int, hi: int, seed: int, dwell_mean: float = 10.0,
     return [step_signal(rng, int(L), 90.0, 12.0, dwell_mean, noise_sd).astype(dtype) for L in lens]
 
 
+def medoid_workload(n_series: int = 2000, len_lo: int = 2000, len_hi: int = 8000,
+                    seed: int = SEED_BASE + 2) -> list[np.ndarray]:
+    """The medoid all-vs-all workload (2000 series by default): lengths uniform
+    in [len_lo, len_hi], piecewise-constant N(90, 12) pA levels with geometric
+    dwells of mean 10 samples plus N(0, 2) noise, float32, sorted by length as
+    performDBA sorts before its medoid pass (dba.hpp:876-885).  Raw values:
+    z-normalisation is the pipeline's first device step."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(len_lo, len_hi + 1, size=n_series)
+    series = []
+    for L in lens:
+        dw = rng.geometric(0.1, size=int(L) // 4 + 16)
+        while dw.sum() < L:
+            dw = np.concatenate([dw, rng.geometric(0.1, size=int(L) // 4 + 16)])
+        levels = rng.normal(90.0, 12.0, size=len(dw))
+        x = np.repeat(levels, dw)[:L] + rng.normal(0.0, 2.0, size=int(L))
+        series.append(x.astype(np.float32))
+    series.sort(key=len)
+    return series
+
+
 def znorm_host(series: list[np.ndarray]) -> list[np.ndarray]:
     """Population z-normalisation in float64, cast back to each series' dtype.
 

@@ -72,6 +72,10 @@ def lib():
             f = getattr(_lib, f"oracle_znorm_{sfx}")
             f.argtypes = [P, P, P, ctypes.c_int, P, P]
             f.restype = ctypes.c_int
+        f = _lib.oracle_pairwise_fp64ref
+        f.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P,
+                      ctypes.c_int64, ctypes.c_int]
+        f.restype = ctypes.c_int
     return _lib
 
 
@@ -132,6 +136,34 @@ def pairwise_fast(series, open_start=0, open_end=0, pair_list=None, threads=0):
         _ptr(pl) if pl is not None else None, 0 if pl is None else len(pl), threads)
     assert rc == 0
     return out
+
+
+def pairwise_fp64ref(series, open_start=0, open_end=0, pair_list=None, threads=0, for_f32=None):
+    """FP64 reference distances (the same recurrence in double, double square
+    root); entries outside pair_list are left 0."""
+    if for_f32 is None:
+        for_f32 = np.dtype(series[0].dtype) == np.float32
+    flat, offsets, lens = pack(series, np.float64)
+    n = len(series)
+    out = np.zeros(n * (n - 1) // 2, dtype=np.float64)
+    pl = None if pair_list is None else np.ascontiguousarray(pair_list, dtype=np.int64)
+    rc = lib().oracle_pairwise_fp64ref(
+        _ptr(flat), _ptr(offsets), _ptr(lens), n, open_start, open_end, int(bool(for_f32)), _ptr(out),
+        _ptr(pl) if pl is not None else None, 0 if pl is None else len(pl), threads)
+    assert rc == 0
+    return out
+
+
+def rel_error(got, ref):
+    """Relative error of results against FP64 reference values: max, median
+    and count (pairs whose reference is 0 compare absolutely)."""
+    got = np.asarray(got, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    den = np.where(ref != 0, np.abs(ref), 1.0)
+    rel = np.abs(got - ref) / den
+    return {"max_rel": float(rel.max()) if rel.size else 0.0,
+            "median_rel": float(np.median(rel)) if rel.size else 0.0,
+            "pairs": int(rel.size)}
 
 
 def medoid(dists, lens):
@@ -206,6 +238,63 @@ def path_triples(centroid, seq, open_start=0, open_end=0, fma_mode=1):
         _ptr(tri), cap)
     assert k >= 0
     return tri[:3 * k].reshape(k, 3)
+
+
+def member_ranges(centroid, members, open_start=0, open_end=0, fma_mode=1):
+    """Per member and centroid index, the first and last member sample index
+    that centroid index receives in updateCentroid's walk (dba.hpp:374-423),
+    as int32 [n, Lc, 2] ((1, 0) where none): the walk of path_triples, with
+    OPEN_RIGHT cells skipped and the start cell added unless NIL_OPEN_RIGHT."""
+    Lc = len(centroid)
+    out = np.zeros((len(members), Lc, 2), dtype=np.int32)
+    out[:, :, 0] = 1
+    for k, seq in enumerate(members):
+        flip = bool(open_end) and Lc < len(seq)  # dba.hpp:497-501
+        tri = path_triples(centroid, seq, open_start, open_end, fma_mode)
+        lo = np.full(Lc, np.iinfo(np.int32).max, dtype=np.int64)
+        hi = np.full(Lc, -1, dtype=np.int64)
+        for i, j, mv in tri[:-1]:
+            if mv == OPEN_RIGHT:
+                continue
+            t, s = (i, j) if flip else (j, i)
+            lo[t] = min(lo[t], s)
+            hi[t] = max(hi[t], s)
+        if tri[-1][2] != NIL_OPEN_RIGHT:
+            lo[0] = min(lo[0], 0)
+            hi[0] = max(hi[0], 0)
+        got = hi >= 0
+        out[k, got, 0] = lo[got]
+        out[k, got, 1] = hi[got]
+    return out
+
+
+def reduce_ranges(centroid, members, ranges):
+    """The ordered centroid update from member ranges: per centroid index the
+    member samples added in T, members in order, each member's samples from
+    its last index down (the order of the reference's single-thread pile-up,
+    dba.hpp:374-423), then sum / count in T and max |old - new| in double of
+    the difference taken in T (dba.hpp:817-836).  Returns (mean, counts,
+    delta)."""
+    centroid = np.asarray(centroid)
+    T = centroid.dtype.type
+    Lc = len(centroid)
+    mean = np.zeros(Lc, dtype=centroid.dtype)
+    counts = np.zeros(Lc, dtype=np.uint32)
+    delta = 0.0
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for t in range(Lc):
+            acc, cnt = T(0), 0
+            for k, seq in enumerate(members):
+                lo, hi = int(ranges[k, t, 0]), int(ranges[k, t, 1])
+                for i in range(hi, lo - 1, -1):
+                    acc = T(acc + seq[i])
+                cnt += max(0, hi - lo + 1)
+            mean[t] = T(acc / T(cnt))
+            counts[t] = cnt
+            d = abs(float(T(centroid[t] - mean[t])))
+            if d > delta:
+                delta = d
+    return mean, counts, delta
 
 
 def znorm(series):
