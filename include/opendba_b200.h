@@ -158,14 +158,23 @@ int odba_dtw_pairlist_f64(const double *series, const uint64_t *offsets, const u
  * after start-up, or a host that owns the device's whole memory budget and
  * gives plugins no allocator): same inputs, outputs and results as
  * odba_dtw_pairwise_f32, but the work counter and swath-edge buffers live in a
- * fixed 64 MiB array inside the library (one per device, held while the
- * library is loaded) instead of a caller workspace.  Limit: max_len up to
- * 2,097,088 samples; longer series are rejected with
- * ODBA_ERR_INVALID_ARGUMENT, and long series run with fewer warps.  The first
- * call on each device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Calls share the array: calls that overlap on the GPU race and must be
- * serialized by the caller. */
+ * fixed 64 MiB array inside the library instead of a caller workspace.
+ *   - The array belongs to a module of its own.  Under CUDA's lazy module
+ *     loading (the default) it is mapped by the first call on each device, so
+ *     that call can itself need 64 MiB of free device memory: make it at
+ *     start-up.  It stays mapped until the context ends.
+ *   - Every lens[i] must be at most max_len (a pair whose first series is
+ *     longer gets NaN).  max_len up to 2,097,088 samples; a larger one is
+ *     rejected with ODBA_ERR_INVALID_ARGUMENT.  Series above about 4,700
+ *     samples run on fewer warps than odba_dtw_pairwise_f32 (59 % of them at
+ *     8,000 samples on a B200), one block of 4 warps above about 1.05 M.
+ *   - Each call looks up the array's device address (cudaGetSymbolAddress)
+ *     unless its stream is capturing, so a device reset between calls is
+ *     fine; a call on a capturing stream needs an earlier call outside
+ *     capture in the same context.  Make the first call before any stream
+ *     capture.
+ *   - Calls share the array: calls that overlap on the GPU (two streams, two
+ *     host threads) race and must be serialized by the caller. */
 int odba_dtw_pairwise_noalloc_f32(const float *series, const uint64_t *offsets,
                                   const uint64_t *lens, int n, uint64_t max_len,
                                   int use_open_start, int use_open_end, float *dists,

@@ -56,6 +56,7 @@ template <>
 struct Num<float> {
   // "max" sentinel of the reference (limits.hpp:40-43) for absent predecessors
   static __device__ __forceinline__ float big() { return FLT_MAX; }
+  static __device__ __forceinline__ float quiet_nan() { return __int_as_float(0x7fc00000); }
   static __device__ __forceinline__ float cell(float d, float m) { return __fmaf_rn(d, d, m); }
   static __device__ __forceinline__ float min2(float a, float b) { return fminf(a, b); }
   static __device__ __forceinline__ float min3(float a, float b, float c) {
@@ -70,6 +71,9 @@ struct Num<float> {
 template <>
 struct Num<double> {
   static __device__ __forceinline__ double big() { return DBL_MAX; }
+  static __device__ __forceinline__ double quiet_nan() {
+    return __longlong_as_double(0x7ff8000000000000ll);
+  }
   static __device__ __forceinline__ double cell(double d, double m) { return __fma_rn(d, d, m); }
   static __device__ __forceinline__ double min2(double a, double b) { return b < a ? b : a; }
   static __device__ __forceinline__ double min3(double a, double b, double c) {

@@ -24,193 +24,9 @@
 #include "dtw_device.cuh"
 #include "dtw_pipe.cuh"
 #include "odba_internal.h"
+#include "pairwise_kernel.cuh"
 
 namespace odba {
-
-namespace {
-
-constexpr int kWarpsPerBlock = 4;
-constexpr int kMinBlocksPerSM = 3;  // 12 warps per SM measured fastest (16 is slower, 20 spills)
-
-template <typename T>
-struct PairwiseArgs {
-  const T *series;
-  const uint64_t *offsets;
-  const uint64_t *lens;
-  int n;
-  unsigned long long pbeg;    // first pair of the range (upper-triangle index)
-  unsigned long long npairs;  // pairs in the range
-  T *dists;
-  unsigned long long *counter;
-  T *edges;
-  unsigned long long edge_stride;  // elements per edge buffer
-  int open_start, open_end;
-};
-
-__device__ __forceinline__ long long row_start(long long s, long long n) {
-  return s * n - s * (s + 1) / 2;
-}
-
-// Upper-triangle pair index -> (s, j).
-__device__ __forceinline__ void pair_of(long long p, long long n, int &s_out, int &j_out) {
-  const double b = 2.0 * double(n) - 1.0;
-  long long s = (long long)((b - sqrt(b * b - 8.0 * double(p))) * 0.5);
-  if (s < 0) s = 0;
-  if (s > n - 2) s = n - 2;
-  while (s + 1 <= n - 2 && row_start(s + 1, n) <= p) ++s;
-  while (s > 0 && row_start(s, n) > p) --s;
-  s_out = int(s);
-  j_out = int(s + 1 + (p - row_start(s, n)));
-}
-
-template <typename T>
-__device__ __forceinline__ T pair_distance(T corner, int m, int n, int os, int oe) {
-  float v;
-  if ((oe && !os) || (!oe && os)) {
-    v = __fdiv_rn(__fsqrt_rn(float(corner)), float(m));
-  } else {
-    v = __fsqrt_rn(float(corner));
-  }
-  return T(v);
-}
-
-template <typename T, int R, bool TRACK>
-__device__ __forceinline__ EdgeStat<T> run_swath(const SwathJob<T> &job, bool last, T &corner) {
-  T col[R];
-  const EdgeStat<T> st = sweep_swath<T, R, NoGate, false, TRACK>(job, col);
-  if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
-  return st;
-}
-
-// The reference's open-end shortcut (dtw.hpp:74-129, open end without open
-// start) is checked on the left edge of every 1024-column reference swath that
-// starts past the last row: if that edge's value on the last row equals its
-// shortcut minimum (ShortcutRows), the swath and all later ones stop and the
-// distance is taken from that value -- from the sentinel it has just stored
-// when the matrix has one row (dtw.hpp:113, 121).  swath_checks_shortcut: the
-// swath [c0, c0 + W) whose right edge is such a left edge.
-template <typename T>
-__device__ __forceinline__ bool swath_checks_shortcut(int c0, int W, int m, int n, bool oe, int r0) {
-  const int cnext = c0 + W;
-  return oe && r0 == 0 && cnext < n && (cnext % kRefSwath) == 0 && cnext > m;
-}
-
-template <typename T>
-__device__ __forceinline__ bool shortcut_fires(const EdgeStat<T> &st, int m, T &corner) {
-  if (st.etop != st.emin) return false;
-  corner = m == 1 ? Num<T>::big() : st.etop;
-  return true;
-}
-
-// Full swaths use RF registers per lane (swath width 32*RF); the last, partial
-// swath uses the smallest multiple of RQ registers that covers it.  TRACK:
-// the pair may take the open-end shortcut (off at compile time for launches
-// without an open end, so that their sweep carries no extra work).
-template <typename T, int RF, int RQ, bool TRACK>
-__device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
-  constexpr int W = 32 * RF;
-  int k = 0;
-  for (int c0 = 0; c0 < job.n; c0 += W, ++k) {
-    const int width = job.n - c0 < W ? job.n - c0 : W;
-    const bool last = c0 + W >= job.n;
-    job.c0 = c0;
-    job.track = TRACK && swath_checks_shortcut<T>(c0, W, job.m, job.n, job.open_end, job.r0);
-    // ping-pong: swath k writes buffer k%2 and reads buffer (k+1)%2
-    job.edge_in = c0 ? ((k & 1) ? e0 : e1) : nullptr;
-    job.edge_out = last ? nullptr : ((k & 1) ? e1 : e0);
-    job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
-    job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
-    const int rneed = (width + 31) / 32;
-    const int rq = (rneed + RQ - 1) / RQ * RQ;
-    EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
-    if (rq >= RF) {
-      st = run_swath<T, RF, TRACK>(job, last, corner);
-    } else {
-      switch (rq / RQ) {
-#define ODBA_CASE(K)                                          \
-  case K:                                                     \
-    if constexpr (K * RQ < RF) st = run_swath<T, K * RQ, TRACK>(job, last, corner); \
-    break;
-        ODBA_CASE(1)
-        ODBA_CASE(2)
-        ODBA_CASE(3)
-        ODBA_CASE(4)
-        ODBA_CASE(5)
-        ODBA_CASE(6)
-        ODBA_CASE(7)
-#undef ODBA_CASE
-        default:
-          break;
-      }
-    }
-    // the next swath's lane 0 reads what this swath's lane 31 wrote
-    __syncwarp();
-    if (TRACK && job.track) {
-      st.emin = __shfl_sync(kFull, st.emin, 31);
-      st.etop = __shfl_sync(kFull, st.etop, 31);
-      if (shortcut_fires<T>(st, job.m, corner)) return;
-    }
-  }
-}
-
-template <typename T, int RF, int RQ, bool TRACK>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
-    pairwise_kernel(PairwiseArgs<T> a) {
-  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
-  const int lane = threadIdx.x & 31;
-  const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  T *e0 = a.edges + slot * 2 * a.edge_stride;
-  T *e1 = e0 + a.edge_stride;
-  for (;;) {
-    unsigned long long q = 0;
-    if (lane == 0) q = atomicAdd(a.counter, 1ull);
-    q = __shfl_sync(kFull, q, 0);
-    if (q >= a.npairs) break;
-    const long long p = (long long)(a.pbeg + a.npairs - 1 - q);
-    int s, j;
-    pair_of(p, a.n, s, j);
-    SwathJob<T> job;
-    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
-    job.x = a.series + a.offsets[s];
-    job.m = int(a.lens[s]);
-    job.y = a.series + a.offsets[j];
-    job.n = int(a.lens[j]);
-    job.r0 = a.open_start ? 1 : 0;
-    job.open_end = a.open_end != 0;
-    T corner = T(0);
-    sweep_pair<T, RF, RQ, TRACK>(job, e0, e1, corner);
-    if (lane == 0) a.dists[p] = pair_distance<T>(corner, job.m, job.n, a.open_start, a.open_end);
-  }
-}
-
-template <typename T>
-struct Tune;
-template <>
-struct Tune<float> {
-  static constexpr int RF = 32, RQ = 4;
-};
-template <>
-struct Tune<double> {
-  static constexpr int RF = 16, RQ = 4;
-};
-
-template <typename T>
-int grid_size() {
-  static int cached[64] = {0};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && cached[dev]) return cached[dev];
-  int sms = 0, per_sm = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ, false>, kWarpsPerBlock * 32, 0);
-  if (per_sm < 1) per_sm = 1;
-  const int g = sms * per_sm;
-  if (dev < 64) cached[dev] = g;
-  return g;
-}
-
-}  // namespace
 
 // Workspace of the one-warp-per-pair launches: the work counter and two edge
 // buffers per resident warp.
@@ -251,104 +67,6 @@ int whole_pairwise_launch(const T *series, const uint64_t *offsets, const uint64
 }
 
 }  // namespace odba
-
-// ---------------------------------------------------------------------------
-// All-pairs DTW without any device allocation.
-//
-// Some callers cannot allocate device memory where they call us: a serving or
-// real-time loop that forbids allocation after start-up (cudaMalloc can
-// synchronize the device and stall unrelated streams, and can fail under
-// memory pressure mid-run), or a host application that owns the device's whole
-// memory budget and gives its plugins no allocator.  For them the work counter
-// and the per-warp swath-edge buffers live in one fixed array in the library's
-// own device memory instead of a caller workspace.  The array exists once per
-// device for as long as the library is loaded; its size caps the longest
-// series and the number of warps that run at once (fewer warps for longer
-// series).  Every call uses the same array: the work counter is cleared at the
-// start of each call, nothing else needs clearing, and calls that overlap on
-// the GPU (two streams, or two host threads) race on it and must be serialized
-// by the caller.
-namespace odba {
-
-constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB per device
-
-static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
-
-namespace {
-
-constexpr int kMaxDevices = 64;
-void *g_noalloc_ptr[kMaxDevices] = {nullptr};
-
-// Looks up (once per device, with that device current) the device address of
-// g_noalloc_scratch; host code must not use the symbol itself as an address.
-int noalloc_scratch_ptr(void **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return fail(ODBA_ERR_CUDA, "cudaGetDevice failed");
-  if (dev < 0 || dev >= kMaxDevices) return fail(ODBA_ERR_UNSUPPORTED_DEVICE, "device index out of range");
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return fail(ODBA_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
-  return ODBA_OK;
-}
-
-template <typename T>
-int pairwise_noalloc(const T *series, const uint64_t *offsets, const uint64_t *lens, int n,
-                     uint64_t max_len, int os, int oe, T *dists, cudaStream_t stream) {
-  if (n < 0 || (n >= 2 && (!series || !offsets || !lens || !dists)))
-    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer or negative series count");
-  if (max_len == 0) return fail(ODBA_ERR_INVALID_ARGUMENT, "max_len must be at least 1");
-  const unsigned long long stride = (max_len + 32 + 31) / 32 * 32;
-  const size_t per_block = size_t(kWarpsPerBlock) * 2 * stride * sizeof(T);
-  const size_t capacity = kNoAllocScratchBytes - 256;
-  if (max_len > (1ull << 31) || per_block > capacity)
-    return fail(ODBA_ERR_INVALID_ARGUMENT,
-                "max_len exceeds the no-allocation limit: the 64 MiB scratch array holds the "
-                "swath edges of one block of warps for series of up to 2,097,088 samples");
-  if (int rc = require_sm100()) return rc;
-  if (n < 2) return ODBA_OK;
-  void *scratch = nullptr;
-  if (int rc = noalloc_scratch_ptr(&scratch)) return rc;
-  int grid = grid_size<T>();
-  const size_t fit = capacity / per_block;
-  if (size_t(grid) > fit) grid = int(fit);
-  PairwiseArgs<T> a;
-  a.series = series;
-  a.offsets = offsets;
-  a.lens = lens;
-  a.n = n;
-  a.pbeg = 0;
-  a.npairs = (unsigned long long)n * (n - 1) / 2;
-  a.dists = dists;
-  a.counter = static_cast<unsigned long long *>(scratch);
-  a.edges = reinterpret_cast<T *>(static_cast<char *>(scratch) + 256);
-  a.edge_stride = stride;
-  a.open_start = os ? 1 : 0;
-  a.open_end = oe ? 1 : 0;
-  // the counter is the only state that must start at zero
-  cudaError_t e = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream);
-  if (e != cudaSuccess) return fail(ODBA_ERR_CUDA, "clearing the work counter failed");
-  if (a.open_end && !a.open_start)
-    pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ, true><<<grid, kWarpsPerBlock * 32, 0, stream>>>(a);
-  else
-    pairwise_kernel<T, Tune<T>::RF, Tune<T>::RQ, false><<<grid, kWarpsPerBlock * 32, 0, stream>>>(a);
-  return check_launch("pairwise DTW kernel (no-allocation variant)");
-}
-
-}  // namespace
-}  // namespace odba
-
-extern "C" int odba_dtw_pairwise_noalloc_f32(const float *series, const uint64_t *offsets,
-                                             const uint64_t *lens, int n, uint64_t max_len,
-                                             int use_open_start, int use_open_end, float *dists,
-                                             void *stream) {
-  return odba::pairwise_noalloc<float>(series, offsets, lens, n, max_len, use_open_start,
-                                       use_open_end, dists, static_cast<cudaStream_t>(stream));
-}
 
 // ---------------------------------------------------------------------------
 // Pairs from a task list: many independent jobs (each its own set of series,
