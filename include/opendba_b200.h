@@ -251,6 +251,41 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
                        int64_t *path_counts, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* ---- one DBA round over several GPUs: ranges, then the ordered reducer --------
+ * The two halves of odba_dba_round_* for a round whose members are dealt to
+ * several GPUs, as DBAUpdate deals them to its devices (dba.hpp:484-486,
+ * currDevice = seq_index % deviceCount) before averaging on the host
+ * (dba.hpp:817-836).  odba_dba_round_ranges_*: path DTW and backtrack
+ * (updateCentroid's walk, dba.hpp:374-423) of this GPU's members; ranges
+ * (device, n * centroid_len pairs of int32) receives, for member k at pair
+ * k * centroid_len + t, the first and last member sample index that centroid
+ * index t receives ((1, 0) if none); same workspace as odba_dba_round_*.
+ * odba_dba_reduce_ranges_*: from all members' ranges (members in the round's
+ * order, gathered from every GPU) and the series, new_centroid, counts and
+ * *delta exactly as odba_dba_round_* computes them (the sums are added in the
+ * reference's order, so the result is bit-identical to the one-GPU round).
+ * ranges must come from odba_dba_round_ranges_* for the same centroid and
+ * members; workspace of odba_dba_reduce_workspace_bytes. */
+int odba_dba_round_ranges_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int32_t *ranges,
+                              void *workspace, size_t workspace_bytes, void *stream);
+int odba_dba_round_ranges_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int32_t *ranges,
+                              void *workspace, size_t workspace_bytes, void *stream);
+size_t odba_dba_reduce_workspace_bytes(int elem_size, int n);
+int odba_dba_reduce_ranges_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                               const uint64_t *offsets, const uint64_t *lens, int n,
+                               int use_open_start, int use_open_end, const int32_t *ranges,
+                               float *new_centroid, uint32_t *counts, double *delta,
+                               void *workspace, size_t workspace_bytes, void *stream);
+int odba_dba_reduce_ranges_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                               const uint64_t *offsets, const uint64_t *lens, int n,
+                               int use_open_start, int use_open_end, const int32_t *ranges,
+                               double *new_centroid, uint32_t *counts, double *delta,
+                               void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- one DBA round in stripe mode ------------------------------------------------
  * Replaces DBAUpdate<T>'s stripe mode (dba.hpp:515-763), used by the
  * reference when a member's path matrix does not fit in device memory.  Same

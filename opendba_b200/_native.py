@@ -68,6 +68,13 @@ SIGNATURES = {
                                  ctypes.c_size_t, P]),
     "odba_dba_round_f64": (I32, [P, U64, P, P, P, P, I32, I32, I32, P, P, P, P, P, P,
                                  ctypes.c_size_t, P]),
+    "odba_dba_round_ranges_f32": (I32, [P, U64, P, P, P, P, I32, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_dba_round_ranges_f64": (I32, [P, U64, P, P, P, P, I32, I32, I32, P, P, ctypes.c_size_t, P]),
+    "odba_dba_reduce_workspace_bytes": (ctypes.c_size_t, [I32, I32]),
+    "odba_dba_reduce_ranges_f32": (I32, [P, U64, P, P, P, I32, I32, I32, P, P, P, P, P,
+                                         ctypes.c_size_t, P]),
+    "odba_dba_reduce_ranges_f64": (I32, [P, U64, P, P, P, I32, I32, I32, P, P, P, P, P,
+                                         ctypes.c_size_t, P]),
     "odba_dba_batch_workspace_bytes": (ctypes.c_size_t, [I32, P, P, I32, P, P, I32]),
     "odba_dba_batch_round_f32": (I32, [P, P, P, P, P, P, I32, I32, P, P, P, P, P, P, I32, P, P, P, P,
                                        P, P, P, P, P, P, ctypes.c_size_t, P]),

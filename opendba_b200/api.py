@@ -73,6 +73,11 @@ class DeviceSeries:
         ln = torch.from_numpy(lens.view(np.int64)).to(device)
         return cls(data, off, ln, lens, flat.dtype)
 
+    def subset(self, begin: int, end: int) -> "DeviceSeries":
+        """Series begin..end-1 as a view sharing this set's device data."""
+        return DeviceSeries(self.data, self.offsets[begin:end], self.lens[begin:end],
+                            self.host_lens[begin:end], self.dtype)
+
     def to_host(self) -> list[np.ndarray]:
         flat = self.data.cpu().numpy()
         offs = self.offsets.cpu().numpy().view(np.uint64)
@@ -198,6 +203,53 @@ def dba_round(centroid, members: DeviceSeries, open_start: int = 0, open_end: in
             paths.append(t[3 * pos:3 * (pos + int(c[k]))].reshape(-1, 3))
             pos += int(h_lens[k]) + Lc + 1
     return mean, counts.view(torch.int32), float(delta.item()), paths
+
+
+def dba_round_ranges(centroid, members: DeviceSeries, open_start: int = 0, open_end: int = 0,
+                     workspace=None, stream=None):
+    """The first half of a DBA round for a share of the members: path DTW and
+    backtrack (odba_dba_round_ranges_*).  Returns an int32 device tensor
+    [n, len(centroid), 2]: per member and centroid index the first and last
+    member sample index it receives ((1, 0): none)."""
+    torch = _torch()
+    Lc = int(centroid.numel())
+    dev = members.data.device
+    h_lens = np.ascontiguousarray(members.host_lens, dtype=np.uint64)
+    if members.n == 0:
+        return torch.zeros((0, Lc, 2), dtype=torch.int32, device=dev)
+    if workspace is None:
+        nbytes = _native.lib().odba_dba_round_workspace_bytes(
+            members.dtype.itemsize, h_lens.ctypes.data_as(ctypes.c_void_p), members.n, Lc,
+            int(open_start), int(open_end))
+        workspace = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    ranges = torch.empty((members.n, Lc, 2), dtype=torch.int32, device=dev)
+    _native.call(f"odba_dba_round_ranges_{_SFX[members.dtype]}", centroid.data_ptr(), Lc,
+                 members.data.data_ptr(), members.offsets.data_ptr(), members.lens.data_ptr(),
+                 h_lens.ctypes.data_as(ctypes.c_void_p), members.n, int(open_start), int(open_end),
+                 ranges.data_ptr(), workspace.data_ptr(), workspace.numel(), _stream_ptr(stream))
+    return ranges
+
+
+def dba_reduce_ranges(centroid, members: DeviceSeries, ranges, open_start: int = 0,
+                      open_end: int = 0, stream=None):
+    """The second half: the ordered reducer over every member's ranges
+    (odba_dba_reduce_ranges_*).  Returns (new_centroid, counts, delta) as the
+    whole round does."""
+    torch = _torch()
+    Lc = int(centroid.numel())
+    dev = members.data.device
+    ws = torch.empty(max(_native.lib().odba_dba_reduce_workspace_bytes(members.dtype.itemsize,
+                                                                        members.n), 1),
+                     dtype=torch.uint8, device=dev)
+    mean = torch.empty(Lc, dtype=members.data.dtype, device=dev)
+    counts = torch.empty(Lc, dtype=torch.int32, device=dev)
+    delta = torch.empty(1, dtype=torch.float64, device=dev)
+    ranges = ranges.contiguous()
+    _native.call(f"odba_dba_reduce_ranges_{_SFX[members.dtype]}", centroid.data_ptr(), Lc,
+                 members.data.data_ptr(), members.offsets.data_ptr(), members.lens.data_ptr(),
+                 members.n, int(open_start), int(open_end), ranges.data_ptr(), mean.data_ptr(),
+                 counts.data_ptr(), delta.data_ptr(), ws.data_ptr(), ws.numel(), _stream_ptr(stream))
+    return mean, counts, float(delta.item())
 
 
 def perform_dba(series, names, output_prefix: str, open_start: int = 0, open_end: int = 0,

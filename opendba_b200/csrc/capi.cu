@@ -183,6 +183,36 @@ int dba_round_checked(const T *centroid, uint64_t Lc, const T *series,
 }
 
 template <typename T>
+int dba_ranges_checked(const T *centroid, uint64_t Lc, const T *series, const uint64_t *offsets,
+                       const uint64_t *lens, const uint64_t *h_lens, int n, int os, int oe,
+                       int32_t *ranges, void *ws, size_t ws_bytes, void *stream) {
+  if (n < 1 || Lc == 0 || !centroid || !series || !offsets || !lens || !h_lens || !ranges || !ws)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer, empty centroid or no members");
+  for (int k = 0; k < n; ++k)
+    if (h_lens[k] == 0 || h_lens[k] > (1ull << 30))
+      return fail(ODBA_ERR_INVALID_ARGUMENT, "member lengths must be in [1, 2^30]");
+  if (Lc > (1ull << 30)) return fail(ODBA_ERR_INVALID_ARGUMENT, "centroid too long");
+  if (int rc = require_sm100()) return rc;
+  return dba_round_ranges_launch<T>(centroid, Lc, series, offsets, lens, h_lens, n, os ? 1 : 0,
+                                    oe ? 1 : 0, reinterpret_cast<int2 *>(ranges), ws, ws_bytes,
+                                    static_cast<cudaStream_t>(stream));
+}
+
+template <typename T>
+int dba_reduce_checked(const T *centroid, uint64_t Lc, const T *series, const uint64_t *offsets,
+                       const uint64_t *lens, int n, int os, int oe, const int32_t *ranges, T *mean,
+                       uint32_t *counts, double *delta, void *ws, size_t ws_bytes, void *stream) {
+  if (n < 1 || Lc == 0 || !centroid || !series || !offsets || !lens || !ranges || !mean ||
+      !counts || !delta || !ws)
+    return fail(ODBA_ERR_INVALID_ARGUMENT, "null pointer, empty centroid or no members");
+  if (Lc > (1ull << 30)) return fail(ODBA_ERR_INVALID_ARGUMENT, "centroid too long");
+  if (int rc = require_sm100()) return rc;
+  return dba_reduce_ranges_launch<T>(centroid, Lc, series, offsets, lens, n, os ? 1 : 0, oe ? 1 : 0,
+                                     reinterpret_cast<const int2 *>(ranges), mean, counts, delta, ws,
+                                     ws_bytes, static_cast<cudaStream_t>(stream));
+}
+
+template <typename T>
 int prefix_chop_checked(const T *prefix, uint64_t P, const T *series, const uint64_t *offsets,
                                const uint64_t *lens, const uint64_t *h_lens, int n, int64_t *chop,
                                int32_t *hist, void *ws, size_t ws_bytes, void *stream) {
@@ -390,6 +420,49 @@ int odba_dba_round_f64(const double *centroid, uint64_t centroid_len, const doub
   return dba_round_checked<double>(centroid, centroid_len, series, offsets, lens, h_lens, n,
                                    use_open_start, use_open_end, new_centroid, counts, delta,
                                    path_triples, path_counts, workspace, workspace_bytes, stream);
+}
+
+int odba_dba_round_ranges_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int32_t *ranges,
+                              void *workspace, size_t workspace_bytes, void *stream) {
+  return dba_ranges_checked<float>(centroid, centroid_len, series, offsets, lens, h_lens, n,
+                                   use_open_start, use_open_end, ranges, workspace, workspace_bytes,
+                                   stream);
+}
+
+int odba_dba_round_ranges_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                              const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                              int n, int use_open_start, int use_open_end, int32_t *ranges,
+                              void *workspace, size_t workspace_bytes, void *stream) {
+  return dba_ranges_checked<double>(centroid, centroid_len, series, offsets, lens, h_lens, n,
+                                    use_open_start, use_open_end, ranges, workspace, workspace_bytes,
+                                    stream);
+}
+
+size_t odba_dba_reduce_workspace_bytes(int elem_size, int n) {
+  if (n < 1) return 0;
+  return elem_size == 8 ? dba_reduce_workspace_bytes<double>(n) : dba_reduce_workspace_bytes<float>(n);
+}
+
+int odba_dba_reduce_ranges_f32(const float *centroid, uint64_t centroid_len, const float *series,
+                               const uint64_t *offsets, const uint64_t *lens, int n,
+                               int use_open_start, int use_open_end, const int32_t *ranges,
+                               float *new_centroid, uint32_t *counts, double *delta,
+                               void *workspace, size_t workspace_bytes, void *stream) {
+  return dba_reduce_checked<float>(centroid, centroid_len, series, offsets, lens, n, use_open_start,
+                                   use_open_end, ranges, new_centroid, counts, delta, workspace,
+                                   workspace_bytes, stream);
+}
+
+int odba_dba_reduce_ranges_f64(const double *centroid, uint64_t centroid_len, const double *series,
+                               const uint64_t *offsets, const uint64_t *lens, int n,
+                               int use_open_start, int use_open_end, const int32_t *ranges,
+                               double *new_centroid, uint32_t *counts, double *delta,
+                               void *workspace, size_t workspace_bytes, void *stream) {
+  return dba_reduce_checked<double>(centroid, centroid_len, series, offsets, lens, n,
+                                    use_open_start, use_open_end, ranges, new_centroid, counts, delta,
+                                    workspace, workspace_bytes, stream);
 }
 
 size_t odba_dba_round_stripe_workspace_bytes(int elem_size, const uint64_t *h_lens, int n,

@@ -736,20 +736,14 @@ size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int
   return round_layout<T>(n, 1, words, ranges, maxm, ms).total;
 }
 
+namespace {
+
+// The descriptors of a one-job round (members 0..n-1 in order, all active)
+// in the workspace, and round arguments pointing at them; outputs unset.
 template <typename T>
-int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint64_t *offsets,
-                     const uint64_t *lens, const uint64_t *h_lens, int n, int os, int oe, T *mean,
-                     uint32_t *counts, double *delta, int32_t *triples, int64_t *triple_counts,
-                     void *ws, size_t ws_bytes, cudaStream_t stream) {
-  unsigned long long words, ranges, maxm;
-  const uint64_t clen = Lc;
-  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
-  int ms = 1;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
-  if (Lc > maxm) maxm = Lc;
-  const RoundLayout L = round_layout<T>(n, 1, words, ranges, maxm, ms);
-  if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA round workspace too small");
-  char *base = static_cast<char *>(ws);
+RoundArgs<T> single_job_round(const T *centroid, uint64_t Lc, const T *series,
+                              const uint64_t *offsets, const uint64_t *lens, int n, int flags,
+                              const RoundLayout &L, char *base, cudaStream_t stream) {
   int *single = reinterpret_cast<int *>(base + L.off_single);
   int *mseries = single, *mjob = single + n, *d_clen = single + 2 * n, *d_flags = single + 2 * n + 1,
       *d_mbeg = single + 2 * n + 2, *d_mend = single + 2 * n + 3;
@@ -772,12 +766,96 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
   a.mjob = mjob;
   a.order = nullptr;
   a.nmem = n;
+  a.means = nullptr;
+  a.counts = nullptr;
+  a.deltas = nullptr;
+  a.triples = nullptr;
+  a.triple_counts = nullptr;
+  return a;
+}
+
+template <typename T>
+RoundLayout single_job_layout(const uint64_t *h_lens, int n, uint64_t Lc, int flags) {
+  unsigned long long words, ranges, maxm;
+  const uint64_t clen = Lc;
+  int ms = 1;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
+  if (Lc > maxm) maxm = Lc;
+  return round_layout<T>(n, 1, words, ranges, maxm, ms);
+}
+
+}  // namespace
+
+template <typename T>
+int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint64_t *offsets,
+                     const uint64_t *lens, const uint64_t *h_lens, int n, int os, int oe, T *mean,
+                     uint32_t *counts, double *delta, int32_t *triples, int64_t *triple_counts,
+                     void *ws, size_t ws_bytes, cudaStream_t stream) {
+  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
+  const RoundLayout L = single_job_layout<T>(h_lens, n, Lc, flags);
+  if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA round workspace too small");
+  char *base = static_cast<char *>(ws);
+  RoundArgs<T> a = single_job_round<T>(centroid, Lc, series, offsets, lens, n, flags, L, base, stream);
   a.means = mean;
   a.counts = counts;
   a.deltas = delta;
   a.triples = triples;
   a.triple_counts = triple_counts;
   return launch_round<T>(a, L, base, int(Lc), stream);
+}
+
+// The first half of a round for a share of the members (a multi-GPU round
+// deals members to ranks): path DTW and backtrack, then every member's
+// per-centroid-index sample ranges copied to ranges_out (member k's at
+// k * Lc; (1, 0) where a centroid index receives nothing).  Same workspace as
+// dba_round_launch.
+template <typename T>
+int dba_round_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
+                            const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                            int n, int os, int oe, int2 *ranges_out, void *ws, size_t ws_bytes,
+                            cudaStream_t stream) {
+  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
+  const RoundLayout L = single_job_layout<T>(h_lens, n, Lc, flags);
+  if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA round workspace too small");
+  char *base = static_cast<char *>(ws);
+  RoundArgs<T> a = single_job_round<T>(centroid, Lc, series, offsets, lens, n, flags, L, base, stream);
+  // the plan clears the job's delta: point it at a spare word of the header
+  a.deltas = reinterpret_cast<double *>(base + L.off_counter + 16);
+  launch_paths<T>(a, L, base, stream);
+  backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
+  cudaMemcpyAsync(ranges_out, a.ranges, size_t(n) * Lc * sizeof(int2), cudaMemcpyDeviceToDevice, stream);
+  return check_launch("DBA round path and backtrack kernels");
+}
+
+template <typename T>
+size_t dba_reduce_workspace_bytes(int n) {
+  return round_layout<T>(n, 1, 0, 0, 1, 0).total;
+}
+
+// The second half: the ordered reducer over all n members' sample ranges
+// (from dba_round_ranges_launch, members in the round's order), giving the
+// new centroid, the pile-up counts and the delta exactly as the whole round
+// does.
+template <typename T>
+int dba_reduce_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
+                             const uint64_t *offsets, const uint64_t *lens, int n, int os, int oe,
+                             const int2 *ranges, T *mean, uint32_t *counts, double *delta, void *ws,
+                             size_t ws_bytes, cudaStream_t stream) {
+  const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
+  const RoundLayout L = round_layout<T>(n, 1, 0, 0, 1, 0);
+  if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "reducer workspace too small");
+  char *base = static_cast<char *>(ws);
+  RoundArgs<T> a = single_job_round<T>(centroid, Lc, series, offsets, lens, n, flags, L, base, stream);
+  a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
+  a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
+  a.rng_off = reinterpret_cast<unsigned long long *>(base + L.off_rng);
+  a.ranges = const_cast<int2 *>(ranges);
+  a.means = mean;
+  a.counts = counts;
+  a.deltas = delta;
+  plan_kernel<T><<<1, 32, 0, stream>>>(a);
+  reduce_kernel<T><<<dim3(unsigned((Lc + 255) / 256), 1), 256, 0, stream>>>(a);
+  return check_launch("DBA reducer kernels");
 }
 
 template <typename T>
@@ -1615,6 +1693,21 @@ template int dba_round_launch<double>(const double *, uint64_t, const double *, 
                                       const uint64_t *, const uint64_t *, int, int, int, double *,
                                       uint32_t *, double *, int32_t *, int64_t *, void *, size_t,
                                       cudaStream_t);
+template int dba_round_ranges_launch<float>(const float *, uint64_t, const float *, const uint64_t *,
+                                            const uint64_t *, const uint64_t *, int, int, int, int2 *,
+                                            void *, size_t, cudaStream_t);
+template int dba_round_ranges_launch<double>(const double *, uint64_t, const double *,
+                                             const uint64_t *, const uint64_t *, const uint64_t *, int,
+                                             int, int, int2 *, void *, size_t, cudaStream_t);
+template size_t dba_reduce_workspace_bytes<float>(int);
+template size_t dba_reduce_workspace_bytes<double>(int);
+template int dba_reduce_ranges_launch<float>(const float *, uint64_t, const float *, const uint64_t *,
+                                             const uint64_t *, int, int, int, const int2 *, float *,
+                                             uint32_t *, double *, void *, size_t, cudaStream_t);
+template int dba_reduce_ranges_launch<double>(const double *, uint64_t, const double *,
+                                              const uint64_t *, const uint64_t *, int, int, int,
+                                              const int2 *, double *, uint32_t *, double *, void *,
+                                              size_t, cudaStream_t);
 template size_t dba_batch_workspace_bytes<float>(const uint64_t *, const int *, int,
                                                  const uint64_t *, const int *, int);
 template size_t dba_batch_workspace_bytes<double>(const uint64_t *, const int *, int,

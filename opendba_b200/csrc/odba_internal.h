@@ -75,6 +75,19 @@ int dba_round_launch(const T *centroid, uint64_t Lc, const T *series, const uint
                      void *ws, size_t ws_bytes, cudaStream_t stream);
 
 template <typename T>
+int dba_round_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
+                            const uint64_t *offsets, const uint64_t *lens, const uint64_t *h_lens,
+                            int n, int os, int oe, int2 *ranges_out, void *ws, size_t ws_bytes,
+                            cudaStream_t stream);
+template <typename T>
+size_t dba_reduce_workspace_bytes(int n);
+template <typename T>
+int dba_reduce_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
+                             const uint64_t *offsets, const uint64_t *lens, int n, int os, int oe,
+                             const int2 *ranges, T *mean, uint32_t *counts, double *delta, void *ws,
+                             size_t ws_bytes, cudaStream_t stream);
+
+template <typename T>
 size_t dba_round_stripe_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe,
                                         int ckpt_rows);
 template <typename T>

@@ -1,5 +1,7 @@
-"""The medoid pass over several GPUs: one process per GPU, pair ranges balanced
-by DTW cell count, one all-gather of the distance triangle.
+"""The medoid pass and DBA rounds over several GPUs: one process per GPU.
+The medoid pass takes pair ranges balanced by DTW cell count and one
+all-gather of the distance triangle; a DBA round takes member blocks balanced
+by cells and one all-gather of per-member sample ranges (below).
 
 The reference deals whole rows of the pair triangle to its devices in turn
 (approximateMedoidIndices, dba.hpp:67-161) and gathers the distances on the
@@ -89,3 +91,65 @@ def medoid_pass_sharded(ds, host_lens, rank: int, world: int, open_start=0, open
     full = gather_triangle(dists[:npairs], ranges, rank, world, group) if world > 1 else dists[:npairs]
     _, med = api.medoid(full, ds, stream=stream)
     return full, med
+
+
+# ---------------------------------------------------------------------------
+# DBA rounds over several GPUs.
+#
+# The reference deals the members of a round to its devices in turn
+# (DBAUpdate, dba.hpp:484-486: currDevice = seq_index % deviceCount) and adds
+# every aligned sample into one centroid sum with atomics.  Float sums depend
+# on their order, so here each rank aligns a contiguous block of members
+# (odba_dba_round_ranges_*: path DTW and backtrack) and emits, per member and
+# centroid index, the range of member samples that index receives; one
+# all-gather gives every rank all members' ranges in the round's member order,
+# and every rank runs the ordered reducer (odba_dba_reduce_ranges_*) over them.
+# The new centroid is therefore bit-identical to the one-GPU round, and every
+# rank holds it for the next round without a broadcast.  An all-reduce of
+# per-rank partial sums would change the rounding.
+
+def member_shards(lens, world: int):
+    """Contiguous [begin, end) member blocks, one per rank, of near-equal DTW
+    cells (every member is aligned to the same centroid, so cells are
+    proportional to the member's length)."""
+    L = np.asarray(lens, dtype=np.float64)
+    n = len(L)
+    if world <= 1 or n == 0:
+        return [(0, n)] + [(n, n)] * max(0, world - 1)
+    cum = np.concatenate([[0.0], np.cumsum(L)])
+    bounds = [0]
+    for r in range(1, world):
+        k = int(np.searchsorted(cum, cum[-1] * r / world, side="left"))
+        bounds.append(min(max(k, bounds[-1]), n))
+    bounds.append(n)
+    return [(bounds[i], bounds[i + 1]) for i in range(world)]
+
+
+def gather_member_ranges(local, shards, rank: int, world: int, group=None):
+    """All ranks' [count, Lc, 2] int32 range blocks, exchanged with one
+    all-gather (blocks padded to the largest); returns [n, Lc, 2] in member
+    order."""
+    import torch
+    import torch.distributed as dist
+    width = max(e - b for b, e in shards)
+    Lc = local.shape[1]
+    mine = torch.zeros((max(width, 1), Lc, 2), dtype=torch.int32, device=local.device)
+    b, e = shards[rank]
+    if e > b:
+        mine[: e - b] = local
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    return torch.cat([parts[r][: re_ - rb] for r, (rb, re_) in enumerate(shards)], dim=0)
+
+
+def dba_round_sharded(centroid, ds, rank: int, world: int, open_start=0, open_end=0, group=None,
+                      stream=None):
+    """One full-path DBA round over all ranks (every rank passes the same
+    centroid and members): (new centroid, counts, delta), the same on every
+    rank and bit-identical to api.dba_round on one GPU."""
+    from . import api
+    shards = member_shards(ds.host_lens, world)
+    b, e = shards[rank]
+    local = api.dba_round_ranges(centroid, ds.subset(b, e), open_start, open_end, stream=stream)
+    full = gather_member_ranges(local, shards, rank, world, group) if world > 1 else local
+    return api.dba_reduce_ranges(centroid, ds, full, open_start, open_end, stream=stream)

@@ -118,3 +118,34 @@ def test_round_open_end_shortcut_fires(env):
         t = O.path_triples(centroid, seq, 0, 1, fma_mode=1)
         assert np.array_equal(paths[k], t.astype(np.int32))
         assert (paths[k][:, 2] == 4).sum() > 1000  # a long OPEN_RIGHT run on the top row
+
+
+@pytest.mark.parametrize("sfx", ["f32", "f64"])
+@pytest.mark.parametrize("mode", list(MODES))
+def test_round_split_into_ranges_and_reduce_equals_whole_round(env, sfx, mode):
+    # the multi-GPU round's two halves on one GPU: members dealt into three
+    # blocks (sharding.member_shards), ranges per block through
+    # odba_dba_round_ranges_*, concatenated in member order, reduced by
+    # odba_dba_reduce_ranges_* -- bit-identical to odba_dba_round_*, and the
+    # ranges equal the oracle's walk
+    torch, api = env
+    from opendba_b200 import sharding
+    os_, oe = MODES[mode]
+    dt = np.float32 if sfx == "f32" else np.float64
+    rng = np.random.default_rng(808 + len(mode))
+    members = [rng.standard_normal(int(L)).astype(dt) for L in rng.integers(200, 2600, size=14)]
+    centroid = rng.standard_normal(1300).astype(dt)
+    ds = api.DeviceSeries.from_host(members)
+    c = torch.from_numpy(centroid).cuda()
+    want_mean, want_counts, want_delta, _ = api.dba_round(c, ds, os_, oe)
+    shards = sharding.member_shards(ds.host_lens, 3)
+    parts = [api.dba_round_ranges(c, ds.subset(b, e), os_, oe) for b, e in shards]
+    ranges = torch.cat(parts, dim=0)
+    assert np.array_equal(ranges.cpu().numpy(), O.member_ranges(centroid, members, os_, oe))
+    mean, counts, delta = api.dba_reduce_ranges(c, ds, ranges, os_, oe)
+    assert np.array_equal(_bits(mean.cpu().numpy()), _bits(want_mean.cpu().numpy()))
+    assert np.array_equal(counts.cpu().numpy(), want_counts.cpu().numpy())
+    assert delta == want_delta
+    mean1, _, delta1 = sharding.dba_round_sharded(c, ds, 0, 1, os_, oe)
+    assert np.array_equal(_bits(mean1.cpu().numpy()), _bits(want_mean.cpu().numpy()))
+    assert delta1 == want_delta
