@@ -141,8 +141,9 @@ __device__ __forceinline__ T cell_rule(T d, T up, T diag, T left, bool top, bool
 // exit.  la / lb: costs of rows a / b one column left of the lane's first
 // column; dg: cost of row a-1 there.  Returns C[ra][c_last] (row a's last
 // column, needed by the next lane).  MASKED steps may hold lanes outside
-// [r0, m) and the top row.
-template <typename T, int R, bool MASKED>
+// [r0, m); with TOP they may also hold the open-end top row (top_a / top_b),
+// without it the caller guarantees they do not (no open end in this sweep).
+template <typename T, int R, bool MASKED, bool TOP = true>
 __device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T xb, T la, T lb,
                                         T dg, bool act_a, bool act_b, bool top_a, bool top_b,
                                         bool fd0) {
@@ -153,8 +154,11 @@ __device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T x
     const T up = col[j];
     const T da = xa - yv[j];
     T va;
-    if (MASKED) {
+    if (MASKED && TOP) {
       va = cell_rule<T>(da, up, a_diag, a_left, top_a, j == 0 && fd0);
+      va = act_a ? va : up;
+    } else if (MASKED) {
+      va = Num<T>::cell(da, Num<T>::min3(up, a_diag, a_left));
       va = act_a ? va : up;
     } else {
       va = Num<T>::cell(da, Num<T>::min3(up, a_diag, a_left));
@@ -163,8 +167,11 @@ __device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T x
     a_left = va;
     const T db = xb - yv[j];
     T vb;
-    if (MASKED) {
+    if (MASKED && TOP) {
       vb = cell_rule<T>(db, va, b_diag, b_left, top_b, j == 0 && fd0);
+      vb = act_b ? vb : va;
+    } else if (MASKED) {
+      vb = Num<T>::cell(db, Num<T>::min3(va, b_diag, b_left));
       vb = act_b ? vb : va;
     } else {
       vb = Num<T>::cell(db, Num<T>::min3(va, b_diag, b_left));
@@ -288,8 +295,12 @@ __device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&c
     const T diag = dg;
     dg = lb;
     const bool act_a = ra >= r0 && ra < m, act_b = ra + 1 >= r0 && ra + 1 < m;
-    a_last = step_rows2<T, R, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
-                                    oe_top && ra == m - 1, oe_top && ra + 1 == m - 1, fd0);
+    if (oe_top)
+      a_last = step_rows2<T, R, true, true>(col, yv, xa, xb, la, lb, diag, act_a, act_b,
+                                            ra == m - 1, ra + 1 == m - 1, fd0);
+    else
+      a_last = step_rows2<T, R, true, false>(col, yv, xa, xb, la, lb, diag, act_a, act_b, false,
+                                             false, false);
     xa_cur = xa;
     xb_cur = xb;
     if (lane31 && has_out) {
