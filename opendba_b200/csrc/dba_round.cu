@@ -35,8 +35,9 @@ namespace odba {
 namespace {
 
 constexpr int kRoundWarps = 4;
-constexpr int kMaxMoveNil = 255, kMoveDiag = 1, kMoveRight = 2, kMoveUp = 3, kMoveOpenRight = 4,
-              kMoveNilOpenRight = 5;
+// move codes of the reference's path matrix (dtw.hpp:10-16); kMoveDiag,
+// kMoveRight and kMoveUp come with the path sweep (dtw_path.cuh)
+constexpr int kMaxMoveNil = 255, kMoveOpenRight = 4, kMoveNilOpenRight = 5;
 
 template <typename T>
 struct PathTune;
@@ -404,7 +405,7 @@ __device__ __forceinline__ bool walk_member_path(const RoundArgs<T> &a, const Me
       } else if (r == 0) {
         mv = c == 0 ? (os ? kMoveNilOpenRight : kMaxMoveNil) : (os ? kMoveOpenRight : kMoveRight);
       } else {
-        mv = int((wv >> (2 * (c - cbeg))) & 3ull);
+        mv = decode_move(wv, c - cbeg);
         if (mv == kMoveRight && oe && r == g.m - 1) mv = kMoveOpenRight;
       }
       if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {
@@ -1313,7 +1314,7 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s, int buf) {
       if (w.r == 0) {
         mv = w.c == 0 ? (os ? kMoveNilOpenRight : kMaxMoveNil) : (os ? kMoveOpenRight : kMoveRight);
       } else {
-        mv = int((wv >> (2 * (w.c - cbeg))) & 3ull);
+        mv = decode_move(wv, w.c - cbeg);
         if (mv == kMoveRight && a.oe && w.r == H - 1) mv = kMoveOpenRight;
       }
       if (mv == kMaxMoveNil || mv == kMoveNilOpenRight) {

@@ -7,27 +7,50 @@
 // over the three candidate costs rounded separately (fma(d, d, pred), or the
 // free predecessor on the open-end top row).  Ties therefore resolve
 // DIAGONAL > UP > RIGHT, i.e. move = DIAGONAL if diag == min, else UP if
-// up == min, else RIGHT.  Moves are 2-bit codes (1 DIAGONAL, 2 RIGHT, 3 UP);
-// the codes the reference derives from position alone (row 0, (0, 0), the
-// open-end OPEN_RIGHT) are rebuilt by the backtrack.
+// up == min, else RIGHT.  Two bits per cell are kept as two bit planes: D
+// (the diagonal candidate equals the minimum) and U (the up candidate does),
+// each set by one compare and one predicated OR of an immediate; decode_move
+// applies the priority.  The codes the reference derives from position alone
+// (row 0, (0, 0), the open-end OPEN_RIGHT) are rebuilt by the backtrack.
 //
 // Path layout per swath: step t, lane l, row slot s (0 = row a, 1 = row b)
-// at 64-bit word ((t * 32 + l) * 2 + s); bit pair 2j holds register j's move.
-// A warp writes 512 contiguous bytes per step.
+// at 64-bit word ((t * 32 + l) * 2 + s); bit j holds register j's D bit and
+// bit 32 + j its U bit.  A warp writes 512 contiguous bytes per step.
 #pragma once
 
 #include "dtw_device.cuh"
 
 namespace odba {
 
-// One cell with its move.  top: open-end top row (right free); fd: the
+// Sets bit J of w if a == b: one compare and one predicated OR of an
+// immediate (no select, no shifted constant in a register).
+template <int J>
+__device__ __forceinline__ void or_bit_if_eq(unsigned &w, float a, float b) {
+  asm("{\n\t.reg .pred p;\n\tsetp.eq.f32 p, %1, %2;\n\t@p or.b32 %0, %0, %3;\n\t}"
+      : "+r"(w)
+      : "f"(a), "f"(b), "n"(1u << J));
+}
+template <int J>
+__device__ __forceinline__ void or_bit_if_eq(unsigned &w, double a, double b) {
+  asm("{\n\t.reg .pred p;\n\tsetp.eq.f64 p, %1, %2;\n\t@p or.b32 %0, %0, %3;\n\t}"
+      : "+r"(w)
+      : "d"(a), "d"(b), "n"(1u << J));
+}
+
+// Move codes the sweep records (dtw.hpp:10-16).
+constexpr int kMoveDiag = 1, kMoveRight = 2, kMoveUp = 3;
+
+// The move of register j from its step word (DIAGONAL > UP > RIGHT).
+__device__ __forceinline__ int decode_move(unsigned long long w, int j) {
+  if ((w >> j) & 1ull) return kMoveDiag;
+  return ((w >> (32 + j)) & 1ull) ? kMoveUp : kMoveRight;
+}
+
+// One cell with its move bits.  top: open-end top row (right free); fd: the
 // reference's swath-left column on that row (diagonal free too).
-// One cell with its move code already shifted into place: the code of
-// register j sits at bit 2*(j % 16) of the 32-bit half word j / 16, so the
-// two selects take the shifted constants and no shift is needed.
 template <typename T, bool MASKED, int J>
-__device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool fd,
-                                       unsigned &bits) {
+__device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool fd, unsigned &pd,
+                                       unsigned &pu) {
   const T uv = Num<T>::cell(d, up);
   T dv = Num<T>::cell(d, diag);
   T rv = Num<T>::cell(d, left);
@@ -36,50 +59,32 @@ __device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool
     dv = (top && fd) ? diag : dv;
   }
   const T v = Num<T>::min3(uv, dv, rv);
-  constexpr int sh = 2 * (J % 16);
-  bits = (dv == v) ? (1u << sh) : ((uv == v) ? (3u << sh) : (2u << sh));
+  or_bit_if_eq<J>(pd, dv, v);
+  or_bit_if_eq<J>(pu, uv, v);
   return v;
 }
 
 template <typename T, int R, bool MASKED, int J = 0>
 struct PathCols {
-  // Columns J.. of one step: cells of rows a and b, the codes of two
-  // consecutive columns joined by one three-input OR per half word.
+  // Column J of one step: the cells of rows a and b.
   static __device__ __forceinline__ void run(T (&col)[R], const T (&yv)[R], T xa, T xb, T &a_left,
                                              T &a_diag, T &b_left, T &b_diag, bool act_a,
                                              bool act_b, bool top_a, bool top_b, bool fd0,
-                                             unsigned (&wa)[2], unsigned (&wb)[2]) {
+                                             unsigned &da, unsigned &ua, unsigned &db,
+                                             unsigned &ub) {
     if constexpr (J < R) {
-      unsigned ca0, cb0, ca1 = 0, cb1 = 0;
-      {
-        const T up = col[J];
-        T va = path_cell<T, MASKED, J>(xa - yv[J], up, a_diag, a_left, top_a, J == 0 && fd0, ca0);
-        if (MASKED) va = act_a ? va : up;
-        a_diag = up;
-        a_left = va;
-        T vb = path_cell<T, MASKED, J>(xb - yv[J], va, b_diag, b_left, top_b, J == 0 && fd0, cb0);
-        if (MASKED) vb = act_b ? vb : va;
-        b_diag = va;
-        b_left = vb;
-        col[J] = vb;
-      }
-      if constexpr (J + 1 < R) {
-        const T up = col[J + 1];
-        T va = path_cell<T, MASKED, J + 1>(xa - yv[J + 1], up, a_diag, a_left, top_a, false, ca1);
-        if (MASKED) va = act_a ? va : up;
-        a_diag = up;
-        a_left = va;
-        T vb = path_cell<T, MASKED, J + 1>(xb - yv[J + 1], va, b_diag, b_left, top_b, false, cb1);
-        if (MASKED) vb = act_b ? vb : va;
-        b_diag = va;
-        b_left = vb;
-        col[J + 1] = vb;
-      }
-      constexpr int h = (J % 32) / 16;  // J and J + 1 share a half word (J even)
-      wa[h] = wa[h] | ca0 | ca1;
-      wb[h] = wb[h] | cb0 | cb1;
-      PathCols<T, R, MASKED, J + 2>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a,
-                                         act_b, top_a, top_b, fd0, wa, wb);
+      const T up = col[J];
+      T va = path_cell<T, MASKED, J>(xa - yv[J], up, a_diag, a_left, top_a, J == 0 && fd0, da, ua);
+      if (MASKED) va = act_a ? va : up;
+      a_diag = up;
+      a_left = va;
+      T vb = path_cell<T, MASKED, J>(xb - yv[J], va, b_diag, b_left, top_b, J == 0 && fd0, db, ub);
+      if (MASKED) vb = act_b ? vb : va;
+      b_diag = va;
+      b_left = vb;
+      col[J] = vb;
+      PathCols<T, R, MASKED, J + 1>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a,
+                                         act_b, top_a, top_b, fd0, da, ua, db, ub);
     }
   }
 };
@@ -91,11 +96,11 @@ __device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa
                                              unsigned long long &wb) {
   T a_left = la, a_diag = dg;
   T b_left = lb, b_diag = la;
-  unsigned ha[2] = {0u, 0u}, hb[2] = {0u, 0u};
+  unsigned da = 0u, ua = 0u, db = 0u, ub = 0u;
   PathCols<T, R, MASKED, 0>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a, act_b,
-                                 top_a, top_b, fd0, ha, hb);
-  wa = (unsigned long long)ha[0] | ((unsigned long long)ha[1] << 32);
-  wb = (unsigned long long)hb[0] | ((unsigned long long)hb[1] << 32);
+                                 top_a, top_b, fd0, da, ua, db, ub);
+  wa = (unsigned long long)da | ((unsigned long long)ua << 32);
+  wb = (unsigned long long)db | ((unsigned long long)ub << 32);
   return a_left;
 }
 
