@@ -20,6 +20,21 @@ of the pair triangle holding ~1/N of the DTW cells
 all-gather of the distance triangle (8 MB), and every rank takes the medoid
 of the full triangle.  The step time is the max over ranks.
 
+After the timed region, on one GPU, the line also carries:
+  parity          the last timed step's distances against the oracle on the
+                  CPU baseline's pair sample (bit for bit), their SHA-256 and
+                  the medoid against the reference's own run on this
+                  workload (tests/golden/ref/c2_medoid_ref.json), and the
+                  device z-normalisation against the oracle's;
+  fp64_error      relative error of those sampled distances against the same
+                  recurrence evaluated in float64;
+  cpu_baseline    the oracle's distance-only C restatement on all host cores;
+  reference_gpu   the reference's own GPU code (its sources built for sm_100a)
+                  on the first 200 rows of the triangle, distances compared;
+  batched_vs_plain, serving   the batched and served forms against the plain
+                  per-job path (opendba_b200/workloads.py); --no-extras drops
+                  them.
+
 ``--impl reference`` times the reference's DTW recurrence restated in C
 (oracle/, OpenMP on all host cores, the reference itself has no CPU
 implementation) on a bounded random sample of the same workload's pairs.
@@ -153,30 +168,123 @@ def cpu_baseline(series, target_secs: float, seed: int = 7):
     rate = float((lens[rows[probe]] * lens[cols[probe]]).sum()) / max(dt, 1e-6)
     per_pair = float((lens[rows] * lens[cols]).mean())
     k = int(max(threads, min(npairs, target_secs * rate / per_pair)))
-    sample = rng.choice(npairs, size=k, replace=False)
+    sample = np.sort(rng.choice(npairs, size=k, replace=False))
     cells = float((lens[rows[sample]] * lens[cols[sample]]).sum())
     t0 = time.perf_counter()
-    O.pairwise_fast(series, 0, 0, pair_list=sample, threads=threads)
+    d = O.pairwise_fast(series, 0, 0, pair_list=sample, threads=threads)
     dt = time.perf_counter() - t0
-    return {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
-            "sample": f"{k} random pairs of the same workload ({cells:.3e} cells, {dt:.1f} s), "
-                      "distance-only C restatement of dtw.hpp:158-239, OpenMP over pairs"}
+    rec = {"value": cells / dt / 1e9, "unit": "GCUPS", "cores": threads, "kind": "port",
+           "sample": f"{k} random pairs of the same workload ({cells:.3e} cells, {dt:.1f} s), "
+                     "distance-only C restatement of dtw.hpp:158-239, OpenMP over pairs"}
+    return rec, sample, d[sample]
+
+
+def fp64_error(series, sample, got):
+    """Relative error of the float32 distances `got` of the pairs `sample`
+    against the FP64 reference (the same recurrence in double, double square
+    root), on all host threads."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    ref = O.pairwise_fp64ref(series, 0, 0, pair_list=sample, threads=os.cpu_count() or 1)[sample]
+    err = O.rel_error(got, ref)
+    err["seconds"] = time.perf_counter() - t0
+    err["reference"] = "DTW recurrence of dtw.hpp:158-239 in float64, square root in float64"
+    return err
+
+
+def c2_golden(n_series):
+    """The reference's own result on this workload (2000 series only), run
+    with the reference's sources built for sm_100a: digest of all distances
+    and the medoid (tests/golden/ref/c2_medoid_ref.json)."""
+    path = os.path.join(ROOT, "tests", "golden", "ref", "c2_medoid_ref.json")
+    if n_series != N_SERIES or not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def reference_gpu(series, ours, rows, device_index):
+    """The reference's own all-pairs launch loop (dba.hpp:67-161, compiled
+    from its sources for sm_100a by oracle/Makefile into oracle/_ref) on the
+    first `rows` rows of the same input, timed by the host clock between two
+    device synchronisations; its distances are compared with ours bit for bit.
+    A context figure: extrapolated to the whole triangle by cells."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return {"unavailable": "oracle/_ref/ref_harness is not built (built from the reference's "
+                               "sources where they are present)"}
+    from oracle import oracle as O
+    with tempfile.TemporaryDirectory() as d:
+        inp, outp = os.path.join(d, "in.odbs"), os.path.join(d, "out.odbs")
+        O.write_bundle(inp, series)
+        with ClockSampler(device_index) as clk:
+            p = subprocess.run([harness, "pairwise", inp, outp, "0", "0", str(rows)],
+                               capture_output=True, text=True, timeout=1200)
+        if p.returncode != 0:
+            return {"unavailable": f"reference harness exited {p.returncode}: {p.stderr[-300:]}"}
+        rec = json.loads(p.stdout.strip().splitlines()[-1])
+        ref = O.read_bundle(outp)[0]
+    n = len(series)
+    k = rows * n - rows * (rows + 1) // 2  # pairs of the first `rows` rows
+    mism = int(np.count_nonzero(ref[:k].view(np.uint32) != ours[:k].view(np.uint32)))
+    total = cells_of([len(s) for s in series])
+    return {"value": rec["gcups"], "unit": "GCUPS", "rows": rows, "pairs": k, "cells": rec["cells"],
+            "seconds": rec["ms"] / 1e3, "clocks": clk.summary(),
+            "full_pass_seconds_extrapolated": total / (rec["gcups"] * 1e9),
+            "distance_mismatches_vs_ours": mism,
+            "basis": f"the reference's DTWDistance launch loop on the first {rows} rows of the triangle "
+                     "(shortest first series against all later ones), host clock between device "
+                     "synchronisations; extrapolated to the full triangle by cells"}
+
+
+def checks_and_baselines(args, series_raw, ds, out, medoid_idx, device_index):
+    """After the timed region (1 GPU): parity of the last timed step's
+    distances and medoid against the oracle's pair sample and the reference's
+    own result on this workload, their error against FP64, the CPU baseline,
+    and the reference's GPU code timed on the same input."""
+    import hashlib
+    from oracle import oracle as O
+    res = {}
+    normed, _, _ = O.znorm(series_raw)
+    ours = out.cpu().numpy()
+    flat = np.concatenate(normed)
+    dev_flat = ds.data[:len(flat)].cpu().numpy()
+    parity = {"znorm_bits_match_oracle": bool(np.array_equal(dev_flat.view(np.uint32),
+                                                             flat.view(np.uint32)))}
+    golden = c2_golden(args.n_series)
+    if golden is not None:
+        parity["distances_sha256_match_ref"] = (
+            hashlib.sha256(ours.tobytes()).hexdigest() == golden["dist_sha256"])
+        parity["medoid_ref"] = golden["medoid"]
+        parity["medoid_matches_ref"] = medoid_idx == golden["medoid"]
+        parity["ref_source"] = ("the reference's sources built for sm_100a, run on this workload "
+                                "(tests/golden/ref/c2_medoid_ref.json)")
+    if not args.no_cpu:
+        cb, sample, cpu_d = cpu_baseline(normed, args.cpu_secs)
+        res["cpu_baseline"] = cb
+        parity["pairs_checked_vs_oracle"] = int(len(sample))
+        parity["mismatches_vs_oracle"] = int(np.count_nonzero(
+            cpu_d.view(np.uint32) != ours[sample].view(np.uint32)))
+        sub = sample[:: max(1, len(sample) // 2000)]  # at most ~2000 pairs in float64
+        res["fp64_error"] = fp64_error(normed, sub, ours[sub])
+    res["parity"] = parity
+    if not args.no_ref_gpu:
+        res["reference_gpu"] = reference_gpu(normed, ours, args.ref_gpu_rows, device_index)
+    return res
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
-    series, _ = workload(0)
-    series = [s for s in series]
-    from opendba_b200 import synth
-    series = synth.znorm_host(series)
+    from oracle import oracle as O
+    series, _, _ = O.znorm(workload(0)[0])
     per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
         cpu_baseline(series, per_step * 0.3, seed=11)
     vals, secs = [], []
     for i in range(args.steps):
         t0 = time.perf_counter()
-        cb = cpu_baseline(series, per_step, seed=100 + i)
+        cb = cpu_baseline(series, per_step, seed=100 + i)[0]
         secs.append(time.perf_counter() - t0)
         vals.append(cb["value"])
     v = float(statistics.mean(vals))
@@ -203,7 +311,7 @@ def extra_results(which):
     if which in ("batched", "all"):
         out["batched_vs_plain"] = workloads.run_batched_vs_plain()
     if which in ("serving", "all"):
-        out["serving"] = [workloads.run_serving(r) for r in (4.0, 64.0)]
+        out["serving"] = workloads.run_serving()
     if which == "long":
         out["long_pairs"] = workloads.run_long()
     if which == "long_round":
@@ -241,22 +349,31 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-secs", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--cpu-secs", type=float, default=30.0,
+                    help="CPU baseline sample budget (30 s: about 1e11 cells on 16 host threads)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="end-to-end steps (default: --steps, at most 5)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the batched-jobs and serving comparisons (about 6 minutes)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="leave out the timing of the reference's own GPU code")
+    ap.add_argument("--ref-gpu-rows", type=int, default=200,
+                    help="rows of the pair triangle the reference's GPU code is timed on")
     ap.add_argument("--n-series", type=int, default=N_SERIES,
                     help="development only: fewer series than the benchmark configuration")
     ap.add_argument("--workload", default="medoid", choices=["medoid", "batched", "serving", "long", "long_round",
                                                              "long_round_open_end", "long_small", "round",
                              "all"],
-                    help="medoid: the metric's configuration (default); batched: many DBA jobs, "
+                    help="medoid: the metric's configuration, with the batched-jobs and serving "
+                         "comparisons unless --no-extras (default; all is the same); batched: many DBA jobs, "
                          "batched vs plain; serving: Poisson request stream, served vs plain; "
                          "long: 16 series of 1M-4M samples, segmentation then all-vs-all f32 and "
                          "f64 and one stripe-mode DBA round (several minutes); long_round: the "
                          "segmentation and the DBA round only (long_round_open_end: that round with "
                          "an open end); round: one full-path DBA round of 400 "
                          "members of 3k-8k samples; long_small: the long workload's all-vs-all "
-                         "with 20k-40k samples (a profiling case); all: the medoid line with batched and serving added")
+                         "with 20k-40k samples (a profiling case)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -336,7 +453,7 @@ def main():
     flat_p = pinned.numpy()
     npairs = len(lens) * (len(lens) - 1) // 2
     dists_h = torch.empty(npairs, dtype=torch.float32).pin_memory().numpy()
-    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else min(args.steps, 5)
     dists_pin = torch.from_numpy(dists_h)
 
     def e2e_step():
@@ -409,9 +526,9 @@ def main():
             "clocks": clocks,
             "medoid": medoid_idx, "medoid_e2e": med_e2e,
         }
-        if world == 1 and not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline(synth.znorm_host(series_raw), args.cpu_secs)
-        if args.workload == "all" and world == 1:
+        if world == 1:
+            line.update(checks_and_baselines(args, series_raw, ds, out, medoid_idx, local))
+        if world == 1 and not args.no_extras:
             line.update(extra_results("all"))
         print(json.dumps(line), flush=True)
     if world > 1:

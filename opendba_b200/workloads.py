@@ -76,6 +76,9 @@ def run_batched_vs_plain(n_jobs=256, count_lo=8, count_hi=512, len_lo=200, len_h
             "cells": cells, "batched_s": tb, "batched_gcups": bg,
             "plain_sample_jobs": len(pick), "plain_sample_cells": pcells, "plain_sample_s": tp,
             "plain_gcups": pg, "speedup": bg / pg, "identical_results_on_sample": bool(same),
+            "plain_basis": (f"sample rate: a seeded sample of {len(pick)} of the {len(jobs)} jobs run "
+                            "one after another through the plain per-job path, cells / seconds on "
+                            "that sample"),
             "rounds_mean": float(np.mean([r["rounds"] for r in res_b])),
             "rounds_max": int(max(r["rounds"] for r in res_b))}
 
@@ -103,85 +106,185 @@ def _request_cells(kind, data, cents, rounds=0, clen=0):
     return job_cells(data, rounds, clen)
 
 
-def run_serving(rate_hz, n_requests=60, seed=0x0DBA0005, budget=32 << 30, detail=False, **kw):
-    """Poisson arrivals through the server; returns latency percentiles and
-    throughput, plus the plain FCFS path on the same requests."""
-    reqs, cents = make_requests(n_requests, seed, **kw)
-    rng = np.random.default_rng(seed + 1)
-    gaps = rng.exponential(1.0 / rate_hz, size=len(reqs))
-    srv = api.Server(np.float32, hbm_budget_bytes=budget)
-    ids = [srv.add_centroid(c) for c in cents]
-    # warm-up
-    w = srv.submit_query([cents[0][:500]], ids[:2])
-    srv.wait(w, 300)
-    srv.take(w)
-    submitted = []
-    t_start = time.perf_counter()
+def _arrival_schedule(n, rate_hz, seed):
+    """Poisson arrival offsets (seconds from the first request's slot)."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0, size=n)) / rate_hz
+
+
+def _drive(offsets, submit):
+    """Calls submit(k) for every request k at its arrival offset (from a
+    producer thread, absolute schedule so the gaps do not drift) and returns
+    the perf_counter time of each submission."""
+    times = [0.0] * len(offsets)
 
     def producer():
-        for (kind, data), g in zip(reqs, gaps):
-            time.sleep(g)
-            rid = srv.submit_query(data, ids) if kind == "q" else srv.submit_job(data)
-            submitted.append((rid, kind, data))
+        t0 = time.perf_counter()
+        for k, off in enumerate(offsets):
+            delay = t0 + off - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            times[k] = time.perf_counter()
+            submit(k)
 
     th = threading.Thread(target=producer)
     th.start()
     th.join()
-    lats, cells, rounds = [], 0.0, []
-    for rid, kind, data in submitted:
-        assert srv.wait(rid, 1200) == 1
-        r = srv.take(rid)
-        lats.append(r["latency_s"])
-        rounds.append(r["rounds"])
-        cells += _request_cells(kind, data, cents, r["rounds"], len(r["result"]) if kind == "j" else 0)
-    wall = time.perf_counter() - t_start
+    return times
+
+
+class PlainServing:
+    """The plain per-job path as a first-come-first-served server, with the
+    same device residency the served path gets: the centroids are uploaded
+    once; each query copies only its reads into a preallocated device buffer,
+    builds its task list with numpy and runs one pair-list launch
+    (odba_dtw_pairlist_f32) on a preallocated workspace; each averaging job
+    runs through the plain drop-in path (odba_dba_jobs_f32, one job)."""
+
+    def __init__(self, reqs, cents):
+        import torch
+        from . import _native
+        self.torch, self.native = torch, _native
+        nc = len(cents)
+        clens = np.array([len(c) for c in cents], dtype=np.uint64)
+        self.nc = nc
+        read_cap = max([sum(len(r) for r in d) for k, d in reqs if k == "q"] + [1])
+        max_first = max([len(r) for k, d in reqs if k == "q" for r in d] + [1])
+        self.ctotal = int(clens.sum())
+        self.data = torch.zeros(self.ctotal + read_cap + 16, dtype=torch.float32, device="cuda")
+        self.data[:self.ctotal].copy_(torch.from_numpy(np.concatenate(cents)))
+        self.host = torch.empty(read_cap, dtype=torch.float32).pin_memory()
+        self.clens = clens
+        self.coffs = np.concatenate([[0], np.cumsum(clens)[:-1]]).astype(np.uint64)
+        max_reads = max([len(d) for k, d in reqs if k == "q"] + [1])
+        self.out = torch.empty(max_reads * nc, dtype=torch.float32, device="cuda")
+        wsz = _native.lib().odba_dtw_pairwise_workspace_bytes(4, max_first)
+        self.ws = torch.empty(wsz, dtype=torch.uint8, device="cuda")
+        self.stream = torch.cuda.current_stream()
+
+    def query(self, reads):
+        torch = self.torch
+        k = len(reads)
+        rl = np.array([len(r) for r in reads], dtype=np.uint64)
+        flat = np.concatenate(reads)
+        self.host[:len(flat)].copy_(torch.from_numpy(flat))
+        self.data[self.ctotal:self.ctotal + len(flat)].copy_(self.host[:len(flat)], non_blocking=True)
+        # series table: centroids 0..nc-1, then the reads (the read is the
+        # first series, as in the serving loop)
+        offs = np.concatenate([self.coffs, self.ctotal + np.concatenate([[0], np.cumsum(rl)[:-1]])])
+        lens = np.concatenate([self.clens, rl])
+        tasks = np.empty(k * self.nc, dtype=[("first", "<u4"), ("second", "<u4"), ("out", "<u8")])
+        tasks["first"] = np.repeat(np.arange(k, dtype=np.uint32) + self.nc, self.nc)
+        tasks["second"] = np.tile(np.arange(self.nc, dtype=np.uint32), k)
+        tasks["out"] = np.arange(k * self.nc, dtype=np.uint64)
+        d_offs = torch.from_numpy(offs.astype(np.uint64).view(np.int64)).cuda()
+        d_lens = torch.from_numpy(lens.astype(np.uint64).view(np.int64)).cuda()
+        d_tasks = torch.from_numpy(tasks.view(np.uint8)).cuda()
+        self.native.call("odba_dtw_pairlist_f32", self.data.data_ptr(), d_offs.data_ptr(),
+                         d_lens.data_ptr(), d_tasks.data_ptr(), k * self.nc, int(rl.max()),
+                         self.out.data_ptr(), self.ws.data_ptr(), self.ws.numel(),
+                         self.stream.cuda_stream)
+        return self.out[:k * self.nc].cpu().numpy()
+
+    def job(self, series):
+        r = api.dba_jobs([series], [0], norm=1, batched=False)[0]
+        return r["centroid"], r["medoid"], r["rounds"]
+
+
+def _pct(v, p):
+    return float(np.percentile(np.asarray(v, dtype=np.float64), p))
+
+
+def run_serving(rates=(8.0, 32.0, 128.0, 512.0), n_requests=300, seed=0x0DBA0005,
+                budget=32 << 30, detail=False, **kw):
+    """Poisson request streams at several arrival rates through the serving
+    loop (continuous batching) and through the plain per-job path run as a
+    first-come-first-served server (PlainServing), same requests, same
+    arrival schedule, both timed by the host clock: latency = completion -
+    arrival per request, throughput = cells / (last completion - first
+    arrival).  Every served result must equal the plain one bit for bit."""
+    import queue
+
+    import torch
+    reqs, cents = make_requests(n_requests, seed, **kw)
+    srv = api.Server(np.float32, hbm_budget_bytes=budget)
+    ids = [srv.add_centroid(c) for c in cents]
+    w = srv.submit_query([cents[0][:500]], ids[:2])  # warm-up
+    srv.wait(w, 300)
+    srv.take(w)
+    plain = PlainServing(reqs, cents)
+    plain.query([cents[0][:500]])  # warm-up (module loading)
+    plain.job([cents[0][:500], cents[1][:600], cents[2][:700]])
+    torch.cuda.synchronize()
+    results = []
+    for rate in rates:
+        offsets = _arrival_schedule(len(reqs), rate, seed + 1)
+        # served: submit at the arrival times, collect afterwards
+        rids = [None] * len(reqs)
+
+        def submit(k):
+            kind, data = reqs[k]
+            rids[k] = srv.submit_query(data, ids) if kind == "q" else srv.submit_job(data)
+
+        sub_t = _drive(offsets, submit)
+        s_lat, s_done, s_res, cells = [], [], [], 0.0
+        for k, rid in enumerate(rids):
+            assert srv.wait(rid, 1200) == 1
+            r = srv.take(rid)
+            s_lat.append(r["latency_s"])
+            s_done.append(sub_t[k] + r["latency_s"])
+            s_res.append(r)
+            kind, data = reqs[k]
+            cells += _request_cells(kind, data, cents, r["rounds"], len(r["result"]) if kind == "j" else 0)
+        s_span = max(s_done) - min(sub_t)
+        # plain: a first-come-first-served consumer fed at the same arrival times
+        q = queue.Queue()
+        arrivals = [0.0] * len(reqs)
+
+        def produce():
+            arrivals[:] = _drive(offsets, q.put)
+
+        prod = threading.Thread(target=produce)
+        prod.start()
+        p_done, same = [0.0] * len(reqs), True
+        for _ in range(len(reqs)):
+            k = q.get()
+            kind, data = reqs[k]
+            if kind == "q":
+                got = plain.query(data)
+                same &= np.array_equal(got.view(np.uint32), s_res[k]["result"].view(np.uint32))
+            else:
+                cen, med, rounds = plain.job(data)
+                same &= (med == s_res[k]["medoid"] and rounds == s_res[k]["rounds"] and
+                         np.array_equal(cen.view(np.uint32), s_res[k]["result"].view(np.uint32)))
+            p_done[k] = time.perf_counter()
+        prod.join()
+        p_lat = [p_done[k] - arrivals[k] for k in range(len(reqs))]
+        p_span = max(p_done) - min(arrivals)
+        rec = {"rate_hz": rate, "requests": len(reqs), "cells": cells,
+               "served": {"gcups": cells / s_span / 1e9, "span_s": s_span,
+                          "p50_ms": 1e3 * _pct(s_lat, 50), "p99_ms": 1e3 * _pct(s_lat, 99)},
+               "plain": {"gcups": cells / p_span / 1e9, "span_s": p_span,
+                         "p50_ms": 1e3 * _pct(p_lat, 50), "p99_ms": 1e3 * _pct(p_lat, 99)},
+               "identical_results": bool(same)}
+        rec["speedup"] = rec["served"]["gcups"] / rec["plain"]["gcups"]
+        if detail:
+            rec["requests_detail"] = [
+                {"kind": kd, "n": len(d), "samples": int(sum(len(x) for x in d)),
+                 "served_ms": 1e3 * sl, "plain_ms": 1e3 * pl}
+                for (kd, d), sl, pl in zip(reqs, s_lat, p_lat)]
+        results.append(rec)
     sstats = srv.stats()
     srv.close()
-    # plain: the same requests one after another through the drop-in paths
-    t0 = time.perf_counter()
-    plain_lat, plain_dur, clock = [], [], 0.0
-    arrivals = np.cumsum(gaps)
-    for (kind, data), arr in zip(reqs, arrivals):
-        s0 = time.perf_counter()
-        if kind == "q":
-            ds = api.DeviceSeries.from_host(list(data) + cents)
-            n = len(data)
-            import torch
-            tasks = np.zeros(n * len(cents), dtype=[("first", "<u4"), ("second", "<u4"), ("out", "<u8")])
-            k = 0
-            for i in range(n):
-                for c in range(len(cents)):
-                    tasks[k] = (i, n + c, k)
-                    k += 1
-            d_tasks = torch.from_numpy(tasks.view(np.uint8)).cuda()
-            out = torch.empty(k, dtype=torch.float32, device="cuda")
-            wsz = api._native.lib().odba_dtw_pairwise_workspace_bytes(4, max(len(r) for r in data))
-            ws = torch.empty(wsz, dtype=torch.uint8, device="cuda")
-            api._native.call("odba_dtw_pairlist_f32", ds.data.data_ptr(), ds.offsets.data_ptr(),
-                             ds.lens.data_ptr(), d_tasks.data_ptr(), k, max(len(r) for r in data),
-                             out.data_ptr(), ws.data_ptr(), ws.numel(),
-                             torch.cuda.current_stream().cuda_stream)
-            out.cpu()
-        else:
-            api.dba_jobs([data], [0], norm=1, batched=False)
-        dur = time.perf_counter() - s0
-        plain_dur.append(dur)
-        clock = max(clock, arr) + dur
-        plain_lat.append(clock - arr)
-    plain_wall = time.perf_counter() - t0
-    pct = lambda v, p: float(np.percentile(np.array(v), p))  # noqa: E731
-    out = {"rate_hz": rate_hz, "requests": len(reqs), "cells": cells,
-            "served_wall_s": wall, "served_gcups": cells / wall / 1e9,
-            "p50_ms": 1e3 * pct(lats, 50), "p99_ms": 1e3 * pct(lats, 99),
-            "plain_busy_s": plain_wall, "plain_gcups": cells / plain_wall / 1e9,
-            "plain_p50_ms": 1e3 * pct(plain_lat, 50), "plain_p99_ms": 1e3 * pct(plain_lat, 99),
-            "server_iterations": sstats["iterations"], "server_busy_s": sstats["busy_s"]}
-    if detail:
-        out["requests_detail"] = [
-            {"kind": k, "n": len(d), "samples": int(sum(len(x) for x in d)), "rounds": rr,
-             "served_ms": 1e3 * l, "plain_ms": 1e3 * pd}
-            for (k, d), rr, l, pd in zip(reqs, rounds, lats, plain_dur)]
-    return out
+    return {"workload": f"{len(reqs)} Poisson requests per rate: 70 % read-vs-centroid queries of 1-64 reads "
+                        "(lengths log-uniform [500,50000]) against 32 resident centroids of 4000 samples, "
+                        "30 % averaging jobs of 16-256 series of 500-2000 samples; float32",
+            "latency": "completion - arrival per request (host clock); throughput: cells / "
+                       "(last completion - first arrival), the same for both arms",
+            "plain": "first-come-first-served: centroids resident, one pair-list launch per query, "
+                     "the plain per-job path per averaging job",
+            "queries": sum(1 for k, _ in reqs if k == "q"), "jobs": sum(1 for k, _ in reqs if k == "j"),
+            "server_iterations": sstats["iterations"], "rates": results}
 
 
 def run_long(n_series=16, len_lo=1_000_000, len_hi=4_000_000, dtypes=("f32", "f64"), minseg=4,
