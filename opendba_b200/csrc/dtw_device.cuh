@@ -183,6 +183,41 @@ __device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T x
   return a_left;
 }
 
+// The unmasked step of step_rows2 in skewed order: row b's cell of column
+// j - 1 comes after row a's cell of column j.  Row a at column j reads
+// C[ra-1][c_{j-1}] (the old col[j-1]) as its diagonal, so in this order the
+// old col[j-1] is dead before row b writes the new col[j-1], and the new value
+// can take the old one's register; in column order every new col[j] would sit
+// in the register of its left neighbour and the whole column would rotate back
+// at the end of each step.  Same cells, same arithmetic, same results.
+template <typename T, int R>
+__device__ __forceinline__ T step_rows2_steady(T (&col)[R], const T (&yv)[R], T xa, T xb, T la,
+                                               T lb, T dg) {
+  T a_left = la, a_diag = dg;
+  T b_left = lb, b_diag = la;
+  T va_prev;
+  {
+    const T up = col[0];
+    va_prev = Num<T>::cell(xa - yv[0], Num<T>::min3(up, a_diag, a_left));
+    a_diag = up;
+    a_left = va_prev;
+  }
+#pragma unroll
+  for (int j = 1; j < R; ++j) {
+    const T up = col[j];
+    const T va = Num<T>::cell(xa - yv[j], Num<T>::min3(up, a_diag, a_left));
+    a_diag = up;
+    a_left = va;
+    const T vb = Num<T>::cell(xb - yv[j - 1], Num<T>::min3(va_prev, b_diag, b_left));
+    b_diag = va_prev;
+    b_left = vb;
+    col[j - 1] = vb;
+    va_prev = va;
+  }
+  col[R - 1] = Num<T>::cell(xb - yv[R - 1], Num<T>::min3(va_prev, b_diag, b_left));
+  return a_left;
+}
+
 template <typename T>
 struct Pair2;
 template <>
@@ -393,8 +428,7 @@ __device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&c
       }
       const T diag = dg;
       dg = lb;
-      a_last = step_rows2<T, R, false>(col, yv, xa, xb, la, lb, diag, true, true, false, false,
-                                       false);
+      a_last = step_rows2_steady<T, R>(col, yv, xa, xb, la, lb, diag);
       xa_cur = xa;
       xb_cur = xb;
       if (CKPT) store_ckpt(r0 + 2 * (t - lane));

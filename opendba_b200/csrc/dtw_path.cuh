@@ -104,6 +104,55 @@ __device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa
   return a_left;
 }
 
+// The unmasked path step in skewed order (see step_rows2_steady in
+// dtw_device.cuh): row b's cell of column J - 1 after row a's cell of column
+// J, so each new col value can take the register of the old one.
+template <typename T, int R, int J>
+struct PathColsSkew {
+  static __device__ __forceinline__ void run(T (&col)[R], const T (&yv)[R], T xa, T xb, T &a_left,
+                                             T &a_diag, T &b_left, T &b_diag, T &va_prev,
+                                             unsigned &da, unsigned &ua, unsigned &db,
+                                             unsigned &ub) {
+    if constexpr (J < R) {
+      const T up = col[J];
+      const T va = path_cell<T, false, J>(xa - yv[J], up, a_diag, a_left, false, false, da, ua);
+      a_diag = up;
+      a_left = va;
+      const T vb = path_cell<T, false, J - 1>(xb - yv[J - 1], va_prev, b_diag, b_left, false, false,
+                                              db, ub);
+      b_diag = va_prev;
+      b_left = vb;
+      col[J - 1] = vb;
+      va_prev = va;
+      PathColsSkew<T, R, J + 1>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, va_prev, da,
+                                     ua, db, ub);
+    }
+  }
+};
+
+template <typename T, int R>
+__device__ __forceinline__ T step_rows2_path_steady(T (&col)[R], const T (&yv)[R], T xa, T xb,
+                                                    T la, T lb, T dg, unsigned long long &wa,
+                                                    unsigned long long &wb) {
+  T a_left = la, a_diag = dg;
+  T b_left = lb, b_diag = la;
+  unsigned da = 0u, ua = 0u, db = 0u, ub = 0u;
+  T va_prev;
+  {
+    const T up = col[0];
+    va_prev = path_cell<T, false, 0>(xa - yv[0], up, a_diag, a_left, false, false, da, ua);
+    a_diag = up;
+    a_left = va_prev;
+  }
+  PathColsSkew<T, R, 1>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, va_prev, da, ua, db,
+                             ub);
+  col[R - 1] = path_cell<T, false, R - 1>(xb - yv[R - 1], va_prev, b_diag, b_left, false, false,
+                                          db, ub);
+  wa = (unsigned long long)da | ((unsigned long long)ua << 32);
+  wb = (unsigned long long)db | ((unsigned long long)ub << 32);
+  return a_left;
+}
+
 struct PathOut {
   unsigned long long *words;  // this swath's move words, (steps * 32 * 2) of them
   bool track_min;             // record min / top of this swath's right-edge column
@@ -309,8 +358,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
       const T diag = dg;
       dg = lb;
       unsigned long long wa, wb;
-      a_last = step_rows2_path<T, R, false>(col, yv, xa, xb, la, lb, diag, true, true, false,
-                                            false, false, wa, wb);
+      a_last = step_rows2_path_steady<T, R>(col, yv, xa, xb, la, lb, diag, wa, wb);
       xa_cur = xa;
       xb_cur = xb;
       ulonglong2 w;
