@@ -554,17 +554,37 @@ __global__ void reduce_kernel(RoundArgs<T> a) {
   if (live && t < Lc) {
     T sum = T(0);
     uint32_t cnt = 0;
-    for (int k = a.mbeg[jb]; k < a.mend[jb]; ++k) {
-      const int2 r = a.ranges[a.rng_off[k] + t];
-      if (r.y < r.x) continue;
-      const T *seq = a.series + a.offsets[a.mseries[k]];
-      for (int i = r.y; i >= r.x; --i) sum = add_rn(sum, seq[i]);
-      cnt += uint32_t(r.y - r.x + 1);
-      if (a.extra) {
-        const int e = a.extra[a.rng_off[k] + t];
-        if (e >= 0) {
-          sum = add_rn(sum, seq[e]);
-          ++cnt;
+    // Members in batches of kBatch: every member's range, series start and
+    // first (highest) sample of the batch are loaded before any of them is
+    // added, so their latencies overlap; the additions keep the order of the
+    // single-member loop (members in order, samples from the highest down,
+    // the stripe-mode extra sample last).
+    constexpr int kBatch = 8;
+    const int kb = a.mbeg[jb], ke = a.mend[jb];
+    for (int k0 = kb; k0 < ke; k0 += kBatch) {
+      int2 r[kBatch];
+      const T *sq[kBatch];
+      T first[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int k = k0 + u;
+        r[u] = k < ke ? a.ranges[a.rng_off[k] + t] : make_int2(1, 0);
+        sq[u] = a.series + (k < ke ? a.offsets[a.mseries[k]] : 0);
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) first[u] = r[u].y >= r[u].x ? sq[u][r[u].y] : T(0);
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        if (r[u].y < r[u].x) continue;
+        sum = add_rn(sum, first[u]);
+        for (int i = r[u].y - 1; i >= r[u].x; --i) sum = add_rn(sum, sq[u][i]);
+        cnt += uint32_t(r[u].y - r[u].x + 1);
+        if (a.extra) {
+          const int e = a.extra[a.rng_off[k0 + u] + t];
+          if (e >= 0) {
+            sum = add_rn(sum, sq[u][e]);
+            ++cnt;
+          }
         }
       }
     }
