@@ -429,9 +429,118 @@ __device__ __forceinline__ bool walk_member_path(const RoundArgs<T> &a, const Me
   }
 }
 
+// The backtrack's ranges alone (no path listing), a row at a time.  In a row
+// the backward walk moves left through RIGHT cells until the first cell whose
+// D or U bit is set; with the row's step word that cell is one
+// count-leading-zeros away, so a row costs a few instructions instead of a
+// few dozen per cell.  The cells that contribute and their order are those of
+// walk_member_path with the backtrack's visitor: the top row's OPEN_RIGHT
+// cells (from the open-end shortcut's column on, and RIGHT on the open-end
+// top row) contribute nothing, row 0 is RIGHT (OPEN_RIGHT with open start)
+// down to (0, 0), which contributes unless it is NIL_OPEN_RIGHT.  With the
+// member on the rows every column of a run is its own centroid index: the
+// columns strictly inside a run receive exactly this row's sample and are
+// stored by all lanes at once.  Returns false if the walk failed.
+template <typename T>
+__device__ __forceinline__ bool walk_member_ranges(const RoundArgs<T> &a, const MemberGeom &g,
+                                                   int k, int os, int oe, int2 *rg) {
+  const int lane = threadIdx.x & 31;
+  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
+  const unsigned long long *w = a.words + a.path_off[k];
+  const int shortcut = a.shortcut[k];
+  const bool lead = lane == 0;
+  int cur_t = -1, lo = 1, hi = 0;
+  auto close = [&]() {
+    if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
+  };
+  auto contribute = [&](int rr, int cc) {
+    const int ti = g.flip ? rr : cc;  // centroid index
+    const int mi = g.flip ? cc : rr;  // member sample index
+    if (ti != cur_t) {
+      close();
+      cur_t = ti;
+      lo = mi;
+      hi = mi;
+    } else {
+      lo = mi;
+    }
+  };
+  // cells (r, c_hi), (r, c_hi - 1), ..., (r, c_lo), in that order
+  auto contribute_run = [&](int r, int c_hi, int c_lo) {
+    if (g.flip) {
+      if (cur_t != r) {
+        close();
+        cur_t = r;
+        hi = c_hi;
+      }
+      lo = c_lo;
+    } else {
+      contribute(r, c_hi);
+      if (c_lo < c_hi) {
+        close();
+        for (int j = c_lo + 1 + lane; j < c_hi; j += 32) rg[j] = make_int2(r, r);
+        cur_t = c_lo;
+        lo = r;
+        hi = r;
+      }
+    }
+  };
+  const long long max_iters = (long long)g.m + g.n + 64;
+  long long iters = 0;
+  int r = g.m - 1, c = g.n - 1;
+  if (shortcut && c >= shortcut) c = shortcut - 1;  // OPEN_RIGHT from the shortcut's column on
+  for (;;) {
+    if (r == 0) {
+      if (!os) contribute_run(0, c, 0);
+      close();
+      return true;
+    }
+    const int s = c / W, c0 = s * W;
+    int R = RF;
+    if (s == g.swaths - 1) {
+      const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
+      R = rq < RF ? rq : RF;
+    }
+    const int top = r, owner = (c - c0) / R, cbeg = c0 + owner * R;
+    unsigned long long word = 0;
+    const int my_row = top - lane;
+    if (my_row >= 1) {
+      const int rr = my_row - g.r0;
+      const unsigned long long t = (unsigned long long)owner + (rr >> 1);
+      word = w[(unsigned long long)s * g.steps * 64ull + (t * 32 + owner) * 2 + (rr & 1)];
+    }
+    for (;;) {
+      if (++iters > max_iters) return false;
+      const unsigned long long wv = __shfl_sync(kFull, word, (top - r) & 31);
+      const unsigned below = 0xffffffffu >> (31 - (c - cbeg));
+      const unsigned du = (unsigned(wv) | unsigned(wv >> 32)) & below;
+      const bool top_open = oe && r == g.m - 1;  // RIGHT there is OPEN_RIGHT
+      if (du == 0) {
+        // RIGHT through the owner's first column: continue in the owner to the left
+        if (!top_open) contribute_run(r, c, cbeg);
+        c = cbeg - 1;
+        if (c < 0) return false;
+        break;
+      }
+      const int jp = 31 - __clz(du);
+      const int cp = cbeg + jp;
+      const bool diag = (unsigned(wv) >> jp) & 1u;
+      if (top_open)
+        contribute(r, cp);
+      else
+        contribute_run(r, c, cp);
+      --r;
+      c = diag ? cp - 1 : cp;
+      if (c < 0) return false;
+      if (r == 0 || top - r >= 32 || c < cbeg) break;  // row 0, or reload the window
+    }
+  }
+}
+
 // The backtrack (updateCentroid's loop, dba.hpp:374-423): per member the
 // contiguous range of member samples each centroid index receives, and the
-// path listing if asked.  One warp per member.
+// path listing if asked.  One warp per member; without a listing the ranges
+// come from walk_member_ranges.
 template <typename T>
 __global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T> a) {
   const int lane = threadIdx.x & 31;
@@ -443,7 +552,11 @@ __global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T
   if (!(flags & 4)) return;
   const int os = flags & 1, oe = (flags >> 1) & 1;
   int2 *rg = a.ranges + a.rng_off[k];
-  int32_t *tri = a.triples ? a.triples + 3ull * a.trip_off[k] : nullptr;
+  if (!a.triples) {
+    walk_member_ranges<T>(a, g, k, os, oe, rg);
+    return;
+  }
+  int32_t *tri = a.triples + 3ull * a.trip_off[k];
   const bool lead = lane == 0;
   long long nt = 0;
   int cur_t = -1, lo = 1, hi = 0;
