@@ -517,47 +517,29 @@ __device__ __forceinline__ bool walk_member_ranges(const RoundArgs<T> &a, const 
       const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
       R = rq < RF ? rq : RF;
     }
-    // The window: rows top .. top - 31, in the columns of the owner lane of c
-    // and of the owner to its left (the previous swath's last owner when c's
-    // owner is its swath's first), two independent loads per lane.
     const int top = r, owner = (c - c0) / R, cbeg = c0 + owner * R;
-    int sl = s, owl = owner - 1, cbegl = cbeg - R;
-    if (owner == 0) {
-      sl = s - 1;
-      owl = 31;
-      cbegl = c0 - RF;  // swaths before the last are full width
-    }
-    const bool has_left = sl >= 0;
-    if (!has_left) cbegl = cbeg;
-    unsigned long long word = 0, wordl = 0;
+    unsigned long long word = 0;
     const int my_row = top - lane;
     if (my_row >= 1) {
       const int rr = my_row - g.r0;
       const unsigned long long t = (unsigned long long)owner + (rr >> 1);
       word = w[(unsigned long long)s * g.steps * 64ull + (t * 32 + owner) * 2 + (rr & 1)];
-      if (has_left) {
-        const unsigned long long tl = (unsigned long long)owl + (rr >> 1);
-        wordl = w[(unsigned long long)sl * g.steps * 64ull + (tl * 32 + owl) * 2 + (rr & 1)];
-      }
     }
     for (;;) {
       if (++iters > max_iters) return false;
-      const bool in_left = c < cbeg;
-      const int base = in_left ? cbegl : cbeg;
-      const unsigned long long wv = __shfl_sync(kFull, in_left ? wordl : word, (top - r) & 31);
-      const unsigned below = 0xffffffffu >> (31 - (c - base));
+      const unsigned long long wv = __shfl_sync(kFull, word, (top - r) & 31);
+      const unsigned below = 0xffffffffu >> (31 - (c - cbeg));
       const unsigned du = (unsigned(wv) | unsigned(wv >> 32)) & below;
       const bool top_open = oe && r == g.m - 1;  // RIGHT there is OPEN_RIGHT
       if (du == 0) {
-        // RIGHT through the owner's first column: on in the owner to the left
-        if (!top_open) contribute_run(r, c, base);
-        c = base - 1;
+        // RIGHT through the owner's first column: continue in the owner to the left
+        if (!top_open) contribute_run(r, c, cbeg);
+        c = cbeg - 1;
         if (c < 0) return false;
-        if (in_left || !has_left) break;  // reload the window
-        continue;
+        break;
       }
       const int jp = 31 - __clz(du);
-      const int cp = base + jp;
+      const int cp = cbeg + jp;
       const bool diag = (unsigned(wv) >> jp) & 1u;
       if (top_open)
         contribute(r, cp);
@@ -566,7 +548,7 @@ __device__ __forceinline__ bool walk_member_ranges(const RoundArgs<T> &a, const 
       --r;
       c = diag ? cp - 1 : cp;
       if (c < 0) return false;
-      if (r == 0 || top - r >= 32 || c < cbegl) break;  // row 0, or reload the window
+      if (r == 0 || top - r >= 32 || c < cbeg) break;  // row 0, or reload the window
     }
   }
 }
