@@ -35,7 +35,6 @@ namespace odba {
 namespace {
 
 constexpr int kRoundWarps = 4;
-constexpr int kMemberMajorSwaths = 32;  // path-pipeline task order, see path_pipe_kernel
 // move codes of the reference's path matrix (dtw.hpp:10-16); kMoveDiag,
 // kMoveRight and kMoveUp come with the path sweep (dtw_path.cuh)
 constexpr int kMaxMoveNil = 255, kMoveOpenRight = 4, kMoveNilOpenRight = 5;
@@ -246,18 +245,11 @@ __device__ __forceinline__ void path_pipe_swath(const SwathJob<T> &job, const Pa
   sweep_swath_path<T, R, PipeGate>(job, po, col, emin, etop, TileIn<T>{nullptr, -1}, gate);
 }
 
-// Path DTW as the swath pipeline: every (member, swath) is one task, so a
-// member's swaths run on different warps at once (few or long members keep
-// the GPU busy); the right edge of swath s goes to buffer s % 2 of the member
-// with one progress word per (member, swath), exactly as in the all-pairs
-// swath pipeline.  Tasks go out member-major (all swaths of the first member
-// in alignment order -- the longest with sorted input -- then the next) when
-// members have at most kMemberMajorSwaths swaths: the tasks that wait for a
-// free warp are then whole short members, a short tail.  With longer chains
-// they go out swath-major (swath 0 of every member, then swath 1, ...), so
-// that no warp holds a late swath long before its predecessor reaches it.
-// Either way a task waits only on its member's previous swath, handed out
-// earlier.  Each swath also stores its
+// Path DTW as the swath pipeline: task k is swath k / nmem of the (k % nmem)-th
+// member in alignment order, so a member's swaths run on different warps at
+// once (few or long members keep the GPU busy); the right edge of swath s goes
+// to buffer s % 2 of the member with one progress word per (member, swath),
+// exactly as in the all-pairs swath pipeline.  Each swath also stores its
 // right edge's minimum and top-row value for the open-end shortcut, which
 // shortcut_kernel resolves afterwards (it never changes a recorded move).
 template <typename T, int RF, int RQ>
@@ -266,20 +258,12 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_pipe_kernel(RoundArgs<T
   constexpr int W = 32 * RF;
   const int lane = threadIdx.x & 31;
   const unsigned long long ntasks = (unsigned long long)a.nmem * a.max_swaths;
-  const bool member_major = a.max_swaths <= kMemberMajorSwaths;
   for (;;) {
     unsigned long long q = 0;
     if (lane == 0) q = atomicAdd(a.counter, 1ull);
     q = __shfl_sync(kFull, q, 0);
     if (q >= ntasks) break;
-    int s, qi;
-    if (member_major) {
-      qi = int(q / a.max_swaths);
-      s = int(q - (unsigned long long)qi * a.max_swaths);
-    } else {
-      s = int(q / a.nmem);
-      qi = int(q - (unsigned long long)s * a.nmem);
-    }
+    const int s = int(q / a.nmem), qi = int(q - (unsigned long long)s * a.nmem);
     const int k = a.order ? a.order[qi] : a.nmem - 1 - qi;
     int jb;
     const MemberGeom g = geom_of<T>(a, k, jb);
