@@ -22,6 +22,7 @@
 // single-thread atomicAdd sequence, without atomics.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <climits>
 #include <cstdint>
 #include <vector>
@@ -738,17 +739,20 @@ __global__ void single_job_kernel(int *mseries, int *mjob, int n, int *clen, int
 
 template <typename T>
 int round_grid() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];  // per device; host threads may race (same value)
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 64 && cached[dev]) return cached[dev];
+  if (dev >= 0 && dev < 64) {
+    const int c = cached[dev].load(std::memory_order_relaxed);
+    if (c) return c;
+  }
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, kRoundWarps>, kRoundWarps * 32, 0);
   if (per_sm < 1) per_sm = 1;
   const int g = sms * per_sm;
-  if (dev < 64) cached[dev] = g;
+  if (dev >= 0 && dev < 64) cached[dev].store(g, std::memory_order_relaxed);
   return g;
 }
 
@@ -1493,10 +1497,13 @@ __global__ void stripe_walk_kernel(StripeArgs<T> a, int s, int buf) {
 
 template <typename T>
 int stripe_grid() {
-  static int cached[64] = {0};
+  static std::atomic<int> cached[64];  // per device; host threads may race (same value)
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 64 && cached[dev]) return cached[dev];
+  if (dev >= 0 && dev < 64) {
+    const int c = cached[dev].load(std::memory_order_relaxed);
+    if (c) return c;
+  }
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -1504,7 +1511,7 @@ int stripe_grid() {
       kRoundWarps * 32, 0);
   if (per_sm < 1) per_sm = 1;
   const int g = sms * per_sm;
-  if (dev < 64) cached[dev] = g;
+  if (dev >= 0 && dev < 64) cached[dev].store(g, std::memory_order_relaxed);
   return g;
 }
 
