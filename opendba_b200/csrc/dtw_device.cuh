@@ -454,278 +454,6 @@ __device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&c
   return st;
 }
 
-// ---------------------------------------------------------------------------
-// Three rows per step: the whole-pair sweep (one warp per pair, no hand-off,
-// no checkpoints).  Lane l at step t works on rows a, b, c = r0 + 3(t - l) +
-// {0, 1, 2}, each row one column behind the one below it, so three dependency
-// chains interleave per lane (two in sweep_swath), and the per-step work of
-// the wavefront (shuffles, lane 0's staged inputs, lane 31's edge stores) is
-// spread over 96 cells instead of 64.  Same cells, same arithmetic, same
-// results as sweep_swath.
-
-constexpr int kChunkRows3 = 96;                      // lane 0's rows per 32 steps
-constexpr int kStageElems3 = 2 * 2 * kChunkRows3;    // two slots of [x | edge]
-
-// Masked step: lanes outside [r0, m) keep their column (act_*), and with TOP
-// the open-end top-row rule applies on the row flagged top_*.  Returns row
-// a's and b's costs at the lane's last column in a_last / b_last.
-template <typename T, int R, bool TOP>
-__device__ __forceinline__ void step_rows3_masked(T (&col)[R], const T (&yv)[R], T xa, T xb, T xc,
-                                                  T la, T lb, T lc, T dg, bool act_a, bool act_b,
-                                                  bool act_c, bool top_a, bool top_b, bool top_c,
-                                                  bool fd0, T &a_last, T &b_last) {
-  T a_left = la, a_diag = dg, b_left = lb, b_diag = la, c_left = lc, c_diag = lb;
-#pragma unroll
-  for (int j = 0; j < R; ++j) {
-    const T up = col[j];
-    T va, vb, vc;
-    if (TOP) {
-      va = cell_rule<T>(xa - yv[j], up, a_diag, a_left, top_a, j == 0 && fd0);
-    } else {
-      va = Num<T>::cell(xa - yv[j], Num<T>::min3(up, a_diag, a_left));
-    }
-    va = act_a ? va : up;
-    a_diag = up;
-    a_left = va;
-    if (TOP) {
-      vb = cell_rule<T>(xb - yv[j], va, b_diag, b_left, top_b, j == 0 && fd0);
-    } else {
-      vb = Num<T>::cell(xb - yv[j], Num<T>::min3(va, b_diag, b_left));
-    }
-    vb = act_b ? vb : va;
-    b_diag = va;
-    b_left = vb;
-    if (TOP) {
-      vc = cell_rule<T>(xc - yv[j], vb, c_diag, c_left, top_c, j == 0 && fd0);
-    } else {
-      vc = Num<T>::cell(xc - yv[j], Num<T>::min3(vb, c_diag, c_left));
-    }
-    vc = act_c ? vc : vb;
-    c_diag = vb;
-    c_left = vc;
-    col[j] = vc;
-  }
-  a_last = a_left;
-  b_last = b_left;
-}
-
-// Steady step, skewed: column j of row a, then column j - 1 of row b, then
-// column j - 2 of row c, so the old col[j - 2] (last read as row a's diagonal
-// at column j - 1) is dead when row c writes the new one.
-template <typename T, int R>
-__device__ __forceinline__ void step_rows3_steady(T (&col)[R], const T (&yv)[R], T xa, T xb, T xc,
-                                                  T la, T lb, T lc, T dg, T &a_last, T &b_last) {
-  T a_left = la, a_diag = dg, b_left = lb, b_diag = la, c_left = lc, c_diag = lb;
-  T va1 = T(0), va2 = T(0), vb1 = T(0);  // row a at j - 1, j - 2; row b at j - 1
-#pragma unroll
-  for (int j = 0; j < R + 2; ++j) {
-    T va = T(0), vb = T(0);
-    if (j < R) {
-      const T up = col[j];
-      va = Num<T>::cell(xa - yv[j], Num<T>::min3(up, a_diag, a_left));
-      a_diag = up;
-      a_left = va;
-    }
-    if (j >= 1 && j - 1 < R) {
-      vb = Num<T>::cell(xb - yv[j - 1], Num<T>::min3(va1, b_diag, b_left));
-      b_diag = va1;
-      b_left = vb;
-    }
-    if (j >= 2) {
-      const T vc = Num<T>::cell(xc - yv[j - 2], Num<T>::min3(vb1, c_diag, c_left));
-      c_diag = vb1;
-      c_left = vc;
-      col[j - 2] = vc;
-    }
-    va2 = va1;
-    va1 = va;
-    vb1 = vb;
-  }
-  (void)va2;
-  a_last = a_left;
-  b_last = b_left;
-}
-
-template <typename T, int R, bool TRACK = true>
-__device__ __forceinline__ EdgeStat<T> sweep_swath3(const SwathJob<T> &job, T (&col)[R]) {
-  const int lane = threadIdx.x & 31;
-  const int m = job.m;
-  const int r0 = job.r0;
-  T yv[R];
-  {
-    const int cl = job.c0 + lane * R;
-#pragma unroll
-    for (int j = 0; j < R; ++j) yv[j] = (cl + j < job.n) ? job.y[cl + j] : T(0);
-  }
-  const T init = r0 ? T(0) : Num<T>::big();
-#pragma unroll
-  for (int j = 0; j < R; ++j) col[j] = init;
-
-  const bool has_in = job.edge_in != nullptr;
-  const bool has_out = job.edge_out != nullptr;
-  const int rows = m - r0;
-  const int total = (rows + 2) / 3 + 31;  // wavefront steps including fill and drain
-  const bool lane0 = lane == 0, lane31 = lane == 31;
-  const bool oe_top = job.open_end && m >= 2;
-  const bool fd0 = job.free_diag0 && lane0;
-  const int last_x = m - 1, last_e = rows > 0 ? rows - 1 : 0;
-
-  T xa_cur = T(0), xb_cur = T(0), xc_cur = T(0), a_last = init, b_last = init;
-  T dg = lane0 ? job.corner_init : init;
-  const bool track = TRACK && job.track && lane31;
-  EdgeStat<T> st{Num<T>::big(), Num<T>::big()};
-  auto note = [&](int r, T v) {
-    if (shortcut_row<T>(r)) st.emin = Num<T>::min2(st.emin, v);
-    if (r == m - 1) st.etop = v;
-  };
-  auto clamp_x = [&](int k) { return r0 + k < last_x ? r0 + k : last_x; };
-  auto clamp_e = [&](int k) { return k < last_e ? k : last_e; };
-
-  // lane 0's inputs of step t: x of rows a, b, c and their left-edge costs
-  auto fetch = [&](int t, T &xa, T &xb, T &xc, T &ea, T &eb, T &ec) {
-    const int k = 3 * t;
-    xa = job.x[clamp_x(k)];
-    xb = job.x[clamp_x(k + 1)];
-    xc = job.x[clamp_x(k + 2)];
-    if (has_in) {
-      ea = job.edge_in[clamp_e(k)];
-      eb = job.edge_in[clamp_e(k + 1)];
-      ec = job.edge_in[clamp_e(k + 2)];
-    } else {
-      ea = eb = ec = Num<T>::big();
-    }
-  };
-
-  auto masked_step = [&](int t) {
-    const int ra = r0 + 3 * (t - lane);
-    T xa = __shfl_up_sync(kFull, xa_cur, 1);
-    T xb = __shfl_up_sync(kFull, xb_cur, 1);
-    T xc = __shfl_up_sync(kFull, xc_cur, 1);
-    T la = __shfl_up_sync(kFull, a_last, 1);
-    T lb = __shfl_up_sync(kFull, b_last, 1);
-    T lc = __shfl_up_sync(kFull, col[R - 1], 1);
-    if (lane0) fetch(t, xa, xb, xc, la, lb, lc);
-    const T diag = dg;
-    dg = lc;
-    const bool act_a = ra >= r0 && ra < m, act_b = ra + 1 >= r0 && ra + 1 < m,
-               act_c = ra + 2 >= r0 && ra + 2 < m;
-    if (oe_top)
-      step_rows3_masked<T, R, true>(col, yv, xa, xb, xc, la, lb, lc, diag, act_a, act_b, act_c,
-                                    ra == m - 1, ra + 1 == m - 1, ra + 2 == m - 1, fd0, a_last,
-                                    b_last);
-    else
-      step_rows3_masked<T, R, false>(col, yv, xa, xb, xc, la, lb, lc, diag, act_a, act_b, act_c,
-                                     false, false, false, false, a_last, b_last);
-    xa_cur = xa;
-    xb_cur = xb;
-    xc_cur = xc;
-    if (lane31 && has_out) {
-      if (act_a) job.edge_out[ra - r0] = a_last;
-      if (act_b) job.edge_out[ra + 1 - r0] = b_last;
-      if (act_c) job.edge_out[ra + 2 - r0] = col[R - 1];
-    }
-    if (track) {
-      if (act_a) note(ra, a_last);
-      if (act_b) note(ra + 1, b_last);
-      if (act_c) note(ra + 2, col[R - 1]);
-    }
-  };
-
-  // chunk c of lane 0's rows (k = ra - r0 in [96c, 96c + 96)) into slot c % 2;
-  // each lane copies rows 3*lane .. 3*lane + 2 of the chunk (clamped like fetch)
-  auto issue_chunk = [&](int c) {
-    T *slot = job.stage + (c & 1) * (2 * kChunkRows3);
-    const int k = c * kChunkRows3 + 3 * lane;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) cp_async_elem(slot + 3 * lane + i, job.x + clamp_x(k + i), sizeof(T));
-    if (has_in) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-        cp_async_elem(slot + kChunkRows3 + 3 * lane + i, job.edge_in + clamp_e(k + i), sizeof(T));
-    }
-    cp_async_commit();
-  };
-  auto staged = [&](int u, T &xa, T &xb, T &xc, T &ea, T &eb, T &ec) {
-    const T *slot = job.stage + ((u >> 5) & 1) * (2 * kChunkRows3);
-    const int i = 3 * (u & 31);
-    xa = slot[i];
-    xb = slot[i + 1];
-    xc = slot[i + 2];
-    if (has_in) {
-      ea = slot[kChunkRows3 + i];
-      eb = slot[kChunkRows3 + i + 1];
-      ec = slot[kChunkRows3 + i + 2];
-    } else {
-      ea = eb = ec = Num<T>::big();
-    }
-  };
-
-  // steady state: rows a, b, c of every lane in [r0, m-2]
-  int steady_end = (rows - 1) / 3;  // first step at which lane 0's row c reaches m-1
-  if (steady_end < 31) steady_end = 31;
-  const int fill_end = total < 31 ? total : 31;
-  int t = 0;
-  for (; t < fill_end; ++t) masked_step(t);
-  if (t < steady_end) {
-    const int cfirst = t >> 5;
-    __syncwarp();
-    issue_chunk(cfirst);
-    issue_chunk(cfirst + 1);
-    cp_async_wait_all();
-    __syncwarp();
-    T pxa = T(0), pxb = T(0), pxc = T(0), pea = T(0), peb = T(0), pec = T(0);
-    if (lane0) staged(t, pxa, pxb, pxc, pea, peb, pec);
-    for (; t < steady_end; ++t) {
-      T xa = __shfl_up_sync(kFull, xa_cur, 1);
-      T xb = __shfl_up_sync(kFull, xb_cur, 1);
-      T xc = __shfl_up_sync(kFull, xc_cur, 1);
-      T la = __shfl_up_sync(kFull, a_last, 1);
-      T lb = __shfl_up_sync(kFull, b_last, 1);
-      T lc = __shfl_up_sync(kFull, col[R - 1], 1);
-      if (((t + 1) & 31) == 0) {
-        // step t + 1 opens chunk c1 (already copied); copy chunk c1 + 1 into
-        // the slot of chunk c1 - 1, whose last read was the previous step's
-        const int c1 = (t + 1) >> 5;
-        cp_async_wait_all();
-        __syncwarp();
-        issue_chunk(c1 + 1);
-      }
-      if (lane0) {
-        xa = pxa;
-        xb = pxb;
-        xc = pxc;
-        la = pea;
-        lb = peb;
-        lc = pec;
-        staged(t + 1, pxa, pxb, pxc, pea, peb, pec);
-      }
-      const T diag = dg;
-      dg = lc;
-      step_rows3_steady<T, R>(col, yv, xa, xb, xc, la, lb, lc, diag, a_last, b_last);
-      xa_cur = xa;
-      xb_cur = xb;
-      xc_cur = xc;
-      if (lane31 && has_out) {
-        T *e = job.edge_out + 3 * (t - 31);
-        e[0] = a_last;
-        e[1] = b_last;
-        e[2] = col[R - 1];
-      }
-      if (track) {
-        const int ra = r0 + 3 * (t - 31);
-        note(ra, a_last);
-        note(ra + 1, b_last);
-        note(ra + 2, col[R - 1]);
-      }
-    }
-    // the next swath reuses the slots: no copy may still be in flight
-    cp_async_wait_all();
-    __syncwarp();
-  }
-  for (; t < total; ++t) masked_step(t);
-  return st;
-}
-
 // Reads the cost at absolute column cabs (which must lie in this swath) from
 // the lane that owns it; every lane returns the value.
 template <typename T, int R>

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     pairlist_kernel(const T *series, const uint64_t *offsets, const uint64_t *lens,
                     const odba_pair_task *tasks, unsigned long long ntasks, T *dists,
                     unsigned long long *counter, T *edges, unsigned long long edge_stride) {
-  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems3];
+  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
   const int lane = threadIdx.x & 31;
   const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   T *e0 = edges + slot * 2 * edge_stride;
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     const int os = int((task.out >> 62) & 1ull), oe = int((task.out >> 63) & 1ull);
     const unsigned long long out = task.out & ((1ull << 62) - 1);
     SwathJob<T> job;
-    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems3;
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     job.x = series + offsets[task.first];
     job.m = int(lens[task.first]);
     job.y = series + offsets[task.second];

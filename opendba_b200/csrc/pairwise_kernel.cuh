@@ -70,7 +70,7 @@ __device__ __forceinline__ T pair_distance(T corner, int m, int n, int os, int o
 template <typename T, int R, bool TRACK>
 __device__ __forceinline__ EdgeStat<T> run_swath(const SwathJob<T> &job, bool last, T &corner) {
   T col[R];
-  const EdgeStat<T> st = sweep_swath3<T, R, TRACK>(job, col);
+  const EdgeStat<T> st = sweep_swath<T, R, NoGate, false, TRACK>(job, col);
   if (last) corner = pick_column<T, R>(col, job.c0, job.n - 1);
   return st;
 }
@@ -149,7 +149,7 @@ __device__ void sweep_pair(SwathJob<T> job, T *e0, T *e1, T &corner) {
 template <typename T, int RF, int RQ, bool TRACK>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     pairwise_kernel(PairwiseArgs<T> a) {
-  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems3];
+  __shared__ __align__(16) T stage_mem[kWarpsPerBlock * kStageElems];
   const int lane = threadIdx.x & 31;
   const long long slot = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
   T *e0 = a.edges + slot * 2 * a.edge_stride;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksPerSM)
     int s, j;
     pair_of(p, a.n, s, j);
     SwathJob<T> job;
-    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems3;
+    job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     job.x = a.series + a.offsets[s];
     job.m = int(a.lens[s]);
     job.y = a.series + a.offsets[j];
