@@ -95,6 +95,10 @@ struct RoundArgs {
   unsigned long long *path_off;  // word offset of member k's path
   unsigned long long *trip_off;  // triple offset of member k's path listing
   unsigned long long *rng_off;   // offset of member k's per-centroid-index ranges
+  // backtrack without a path listing: per member, per row, the column
+  // interval of the row's contributing cells (runs_off[k] = member k's first)
+  unsigned long long *runs_off = nullptr;
+  int2 *runs = nullptr;
   int *shortcut;                 // first column of the open-end shortcut, or 0
   int2 *ranges;
   T *edges;
@@ -131,17 +135,19 @@ __device__ __forceinline__ MemberGeom geom_of(const RoundArgs<T> &a, int k, int 
 template <typename T>
 __global__ void plan_kernel(RoundArgs<T> a) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned long long w = 0, p = 0, r = 0;
+  unsigned long long w = 0, p = 0, r = 0, rr = 0;
   for (int k = 0; k < a.nmem; ++k) {
     int job;
     const MemberGeom g = geom_of<T>(a, k, job);
     a.path_off[k] = w;
     a.trip_off[k] = p;
     a.rng_off[k] = r;
+    if (a.runs_off) a.runs_off[k] = rr;
     p += (unsigned long long)(g.m + g.n + 1);
     if (!(a.jflags[job] & 4)) continue;
     w += g.words;
     r += (unsigned long long)a.clen[job];
+    rr += (unsigned long long)g.m;
   }
   for (int j = 0; j < a.njobs; ++j)
     if (a.jflags[j] & 4) a.deltas[j] = 0.0;
@@ -430,70 +436,34 @@ __device__ __forceinline__ bool walk_member_path(const RoundArgs<T> &a, const Me
   }
 }
 
-// The backtrack's ranges alone (no path listing), a row at a time.  In a row
-// the backward walk moves left through RIGHT cells until the first cell whose
-// D or U bit is set; with the row's step word that cell is one
-// count-leading-zeros away, so a row costs a few instructions instead of a
-// few dozen per cell.  The cells that contribute and their order are those of
-// walk_member_path with the backtrack's visitor: the top row's OPEN_RIGHT
-// cells (from the open-end shortcut's column on, and RIGHT on the open-end
-// top row) contribute nothing, row 0 is RIGHT (OPEN_RIGHT with open start)
-// down to (0, 0), which contributes unless it is NIL_OPEN_RIGHT.  With the
-// member on the rows every column of a run is its own centroid index: the
-// columns strictly inside a run receive exactly this row's sample and are
-// stored by all lanes at once.  Returns false if the walk failed.
+// The backtrack's ranges alone (no path listing), in two passes.  Pass 1 (one
+// warp per member) walks the path a row at a time: in a row the backward walk
+// moves left through RIGHT cells until the first cell whose D or U bit is set,
+// one count-leading-zeros on the row's step word away, and the walk stores
+// the row's interval of contributing cells' columns at runs[r] ((1, 0) if
+// none).  The contributing cells are those of walk_member_path with the
+// backtrack's visitor: the top row's OPEN_RIGHT cells (from the open-end
+// shortcut's column on, and RIGHT on the open-end top row) contribute
+// nothing, so that row contributes only its last cell; row 0 is RIGHT
+// (OPEN_RIGHT with open start) down to (0, 0), which contributes unless it is
+// NIL_OPEN_RIGHT.  Pass 2 (runs_to_ranges_kernel) turns the intervals into
+// per-centroid-index ranges in parallel.  Returns false if the walk failed.
 template <typename T>
-__device__ __forceinline__ bool walk_member_ranges(const RoundArgs<T> &a, const MemberGeom &g,
-                                                   int k, int os, int oe, int2 *rg) {
+__device__ __forceinline__ bool walk_member_runs(const RoundArgs<T> &a, const MemberGeom &g, int k,
+                                                 int os, int oe, int2 *runs) {
   const int lane = threadIdx.x & 31;
   constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
   const bool lead = lane == 0;
-  int cur_t = -1, lo = 1, hi = 0;
-  auto close = [&]() {
-    if (lead && cur_t >= 0 && hi >= lo) rg[cur_t] = make_int2(lo, hi);
-  };
-  auto contribute = [&](int rr, int cc) {
-    const int ti = g.flip ? rr : cc;  // centroid index
-    const int mi = g.flip ? cc : rr;  // member sample index
-    if (ti != cur_t) {
-      close();
-      cur_t = ti;
-      lo = mi;
-      hi = mi;
-    } else {
-      lo = mi;
-    }
-  };
-  // cells (r, c_hi), (r, c_hi - 1), ..., (r, c_lo), in that order
-  auto contribute_run = [&](int r, int c_hi, int c_lo) {
-    if (g.flip) {
-      if (cur_t != r) {
-        close();
-        cur_t = r;
-        hi = c_hi;
-      }
-      lo = c_lo;
-    } else {
-      contribute(r, c_hi);
-      if (c_lo < c_hi) {
-        close();
-        for (int j = c_lo + 1 + lane; j < c_hi; j += 32) rg[j] = make_int2(r, r);
-        cur_t = c_lo;
-        lo = r;
-        hi = r;
-      }
-    }
-  };
   const long long max_iters = (long long)g.m + g.n + 64;
   long long iters = 0;
   int r = g.m - 1, c = g.n - 1;
   if (shortcut && c >= shortcut) c = shortcut - 1;  // OPEN_RIGHT from the shortcut's column on
+  int entry = c;                                    // the column the walk entered row r at
   for (;;) {
     if (r == 0) {
-      if (!os) contribute_run(0, c, 0);
-      close();
+      if (lead) runs[0] = os ? make_int2(1, 0) : make_int2(0, c);
       return true;
     }
     const int s = c / W, c0 = s * W;
@@ -515,10 +485,8 @@ __device__ __forceinline__ bool walk_member_ranges(const RoundArgs<T> &a, const 
       const unsigned long long wv = __shfl_sync(kFull, word, (top - r) & 31);
       const unsigned below = 0xffffffffu >> (31 - (c - cbeg));
       const unsigned du = (unsigned(wv) | unsigned(wv >> 32)) & below;
-      const bool top_open = oe && r == g.m - 1;  // RIGHT there is OPEN_RIGHT
       if (du == 0) {
-        // RIGHT through the owner's first column: continue in the owner to the left
-        if (!top_open) contribute_run(r, c, cbeg);
+        // RIGHT through the owner's first column: on in the owner to the left
         c = cbeg - 1;
         if (c < 0) return false;
         break;
@@ -526,22 +494,54 @@ __device__ __forceinline__ bool walk_member_ranges(const RoundArgs<T> &a, const 
       const int jp = 31 - __clz(du);
       const int cp = cbeg + jp;
       const bool diag = (unsigned(wv) >> jp) & 1u;
-      if (top_open)
-        contribute(r, cp);
-      else
-        contribute_run(r, c, cp);
+      if (lead) runs[r] = make_int2(cp, (oe && r == g.m - 1) ? cp : entry);
       --r;
       c = diag ? cp - 1 : cp;
+      entry = c;
       if (c < 0) return false;
       if (r == 0 || top - r >= 32 || c < cbeg) break;  // row 0, or reload the window
     }
   }
 }
 
+// Pass 2, one block per member: the contributing columns of row r are the
+// interval runs[r] = [x, y].  Member on the rows (centroid index t = column):
+// column t's range is [lowest, highest] row holding t.  Consecutive rows'
+// intervals share at most one column -- row r's first with row r - 1's last
+// (an UP move) and row r's last with row r + 1's first -- so row r stores a
+// column's high end unless row r + 1 also holds it and its low end unless row
+// r - 1 also holds it; every other column of the interval is row r's alone.
+// Centroid on the rows (t = row): the interval is the range.
+template <typename T>
+__global__ void runs_to_ranges_kernel(RoundArgs<T> a) {
+  const int k = blockIdx.x;
+  int jb;
+  const MemberGeom g = geom_of<T>(a, k, jb);
+  if (!(a.jflags[jb] & 4)) return;
+  const int2 *runs = a.runs + a.runs_off[k];
+  int2 *rg = a.ranges + a.rng_off[k];
+  for (int r = threadIdx.x; r < g.m; r += blockDim.x) {
+    const int2 iv = runs[r];
+    if (iv.x > iv.y) continue;
+    if (g.flip) {
+      rg[r] = iv;
+      continue;
+    }
+    const int2 above = r + 1 < g.m ? runs[r + 1] : make_int2(1, 0);
+    const int2 below = r > 0 ? runs[r - 1] : make_int2(1, 0);
+    const bool top_shared = above.x <= iv.y && iv.y <= above.y;
+    const bool low_shared = below.x <= iv.x && iv.x <= below.y;
+    for (int t = iv.x; t <= iv.y; ++t) {
+      if (!(t == iv.y && top_shared)) rg[t].y = r;
+      if (!(t == iv.x && low_shared)) rg[t].x = r;
+    }
+  }
+}
+
 // The backtrack (updateCentroid's loop, dba.hpp:374-423): per member the
 // contiguous range of member samples each centroid index receives, and the
-// path listing if asked.  One warp per member; without a listing the ranges
-// come from walk_member_ranges.
+// path listing if asked.  One warp per member; without a listing it runs pass
+// 1 of the two-pass ranges (walk_member_runs; launch_backtrack adds pass 2).
 template <typename T>
 __global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T> a) {
   const int lane = threadIdx.x & 31;
@@ -554,7 +554,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32) backtrack_kernel(RoundArgs<T
   const int os = flags & 1, oe = (flags >> 1) & 1;
   int2 *rg = a.ranges + a.rng_off[k];
   if (!a.triples) {
-    walk_member_ranges<T>(a, g, k, os, oe, rg);
+    walk_member_runs<T>(a, g, k, os, oe, a.runs + a.runs_off[k]);
     return;
   }
   int32_t *tri = a.triples + 3ull * a.trip_off[k];
@@ -757,8 +757,8 @@ int round_grid() {
 }
 
 struct RoundLayout {
-  size_t off_counter, off_path, off_trip, off_rng, off_short, off_single, off_ranges, off_edges,
-      off_words, off_prog, off_emtop, total;
+  size_t off_counter, off_path, off_trip, off_rng, off_runoff, off_short, off_single, off_ranges,
+      off_runs, off_edges, off_words, off_prog, off_emtop, total;
   unsigned long long edge_stride;
   int max_swaths;
   bool pipe;  // path DTW as the swath pipeline (two edge columns per member)
@@ -769,7 +769,8 @@ constexpr size_t kPipeEdgeBytes = size_t(8) << 30;  // per-member edge columns u
 // Workspace layout for nmem members / njobs jobs with the given totals.
 template <typename T>
 RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
-                         unsigned long long ranges, unsigned long long maxm, int max_swaths = 0) {
+                         unsigned long long ranges, unsigned long long maxm, int max_swaths = 0,
+                         unsigned long long rows = 0) {
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   RoundLayout L;
   L.edge_stride = (maxm + 32 + 31) / 32 * 32;
@@ -782,10 +783,12 @@ RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
   L.off_path = o; o += up(size_t(nmem) * 8);
   L.off_trip = o; o += up(size_t(nmem) * 8);
   L.off_rng = o; o += up(size_t(nmem) * 8);
+  L.off_runoff = o; o += up(size_t(nmem) * 8);
   L.off_short = o; o += up(size_t(nmem) * 4);
   // single-job descriptors: mseries, mjob (nmem ints each), clen, jflags, mbeg, mend, coff
   L.off_single = o; o += up(size_t(nmem) * 8 + 64);
   L.off_ranges = o; o += up(size_t(ranges) * sizeof(int2));
+  L.off_runs = o; o += up(size_t(rows) * sizeof(int2));  // cleared with the ranges
   L.off_edges = o; o += up(edge_cols * 2 * L.edge_stride * sizeof(T));
   L.off_words = o; o += up(words * 8);
   const size_t ps = L.pipe ? size_t(nmem) * size_t(max_swaths) : 0;
@@ -799,10 +802,12 @@ RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
 template <typename T>
 void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint64_t *h_clen,
                  const int *h_flags, unsigned long long &words, unsigned long long &ranges,
-                 unsigned long long &maxm, int *max_swaths = nullptr) {
+                 unsigned long long &maxm, int *max_swaths = nullptr,
+                 unsigned long long *rows = nullptr) {
   words = ranges = 0;
   maxm = 1;
   if (max_swaths) *max_swaths = 1;
+  if (rows) *rows = 0;
   for (int k = 0; k < nmem; ++k) {
     const int j = h_mjob ? h_mjob[k] : 0;
     const int f = h_flags[j];
@@ -812,6 +817,7 @@ void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint
     ranges += h_clen[j];
     if ((unsigned long long)g.m > maxm) maxm = g.m;
     if (max_swaths && g.swaths > *max_swaths) *max_swaths = g.swaths;
+    if (rows) *rows += (unsigned long long)g.m;
   }
 }
 
@@ -823,8 +829,10 @@ void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_
   a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
   a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
   a.rng_off = reinterpret_cast<unsigned long long *>(base + L.off_rng);
+  a.runs_off = reinterpret_cast<unsigned long long *>(base + L.off_runoff);
   a.shortcut = reinterpret_cast<int *>(base + L.off_short);
   a.ranges = reinterpret_cast<int2 *>(base + L.off_ranges);
+  a.runs = reinterpret_cast<int2 *>(base + L.off_runs);
   a.edges = reinterpret_cast<T *>(base + L.off_edges);
   a.edge_stride = L.edge_stride;
   a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
@@ -851,11 +859,20 @@ void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_
         <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
 }
 
+// The backtrack: with a path listing one kernel walking cell by cell; without,
+// the row walk (pass 1) and the parallel conversion of its row intervals into
+// ranges (pass 2).
+template <typename T>
+void launch_backtrack(const RoundArgs<T> &a, cudaStream_t stream) {
+  backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
+  if (!a.triples) runs_to_ranges_kernel<T><<<a.nmem, 256, 0, stream>>>(a);
+}
+
 template <typename T>
 int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen,
                  cudaStream_t stream) {
   launch_paths<T>(a, L, base, stream);
-  backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
+  launch_backtrack<T>(a, stream);
   dim3 rg((max_clen + 255) / 256, a.njobs);
   reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
   return check_launch("DBA round kernels");
@@ -869,9 +886,10 @@ size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int
   const uint64_t clen = Lc;
   const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
   int ms = 1;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
+  unsigned long long rows = 0;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms, &rows);
   if (Lc > maxm) maxm = Lc;
-  return round_layout<T>(n, 1, words, ranges, maxm, ms).total;
+  return round_layout<T>(n, 1, words, ranges, maxm, ms, rows).total;
 }
 
 namespace {
@@ -917,9 +935,10 @@ RoundLayout single_job_layout(const uint64_t *h_lens, int n, uint64_t Lc, int fl
   unsigned long long words, ranges, maxm;
   const uint64_t clen = Lc;
   int ms = 1;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms);
+  unsigned long long rows = 0;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms, &rows);
   if (Lc > maxm) maxm = Lc;
-  return round_layout<T>(n, 1, words, ranges, maxm, ms);
+  return round_layout<T>(n, 1, words, ranges, maxm, ms, rows);
 }
 
 }  // namespace
@@ -960,7 +979,7 @@ int dba_round_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
   // the plan clears the job's delta: point it at a spare word of the header
   a.deltas = reinterpret_cast<double *>(base + L.off_counter + 16);
   launch_paths<T>(a, L, base, stream);
-  backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
+  launch_backtrack<T>(a, stream);
   cudaMemcpyAsync(ranges_out, a.ranges, size_t(n) * Lc * sizeof(int2), cudaMemcpyDeviceToDevice, stream);
   return check_launch("DBA round path and backtrack kernels");
 }
@@ -1001,10 +1020,11 @@ size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int
                                  const uint64_t *h_clen, const int *h_flags, int njobs) {
   unsigned long long words, ranges, maxm;
   int ms = 1;
-  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms);
+  unsigned long long rows = 0;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms, &rows);
   for (int j = 0; j < njobs; ++j)
     if (h_clen[j] > maxm) maxm = h_clen[j];
-  return round_layout<T>(nmem, njobs, words, ranges, maxm, ms).total;
+  return round_layout<T>(nmem, njobs, words, ranges, maxm, ms, rows).total;
 }
 
 template <typename T>
@@ -1018,10 +1038,11 @@ int dba_batch_launch(const T *centroids, const unsigned long long *coff, const i
                      cudaStream_t stream) {
   unsigned long long words, ranges, maxm;
   int ms = 1;
-  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms);
+  unsigned long long rows = 0;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms, &rows);
   for (int j = 0; j < njobs; ++j)
     if (h_clen[j] > maxm) maxm = h_clen[j];
-  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm, ms);
+  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm, ms, rows);
   if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA batch workspace too small");
   RoundArgs<T> a;
   a.centroids = centroids;
