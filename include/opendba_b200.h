@@ -121,6 +121,16 @@ int odba_tune_flush(void);
 int odba_tune_save(const char *path);
 int odba_tune_load(const char *path);
 
+/* ---- row bands of the DBA round's path DTW ----------------------------------------
+ * No reference counterpart (a tuning knob; results do not depend on it).
+ * When a round's (member, swath) tasks are fewer than about three waves of
+ * the GPU's resident warps, the path DTW cuts each member's rows into bands
+ * so that the last wave of tasks is short.  n in 1..8 pins the number of
+ * bands for the following launches (1: none), 0 restores the automatic
+ * choice.  A workspace size queried under one setting fits launches under the
+ * same setting. */
+int odba_round_set_bands(int n);
+
 /* ---- self-test of the bounded device wait --------------------------------------
  * No reference counterpart.  One warp runs the swath pipeline's wait on a
  * progress word that nothing publishes, with the given limit (at most 10 s);

@@ -43,6 +43,7 @@ SIGNATURES = {
     "odba_prefix_chop_f32": (I32, [P, U64, P, P, P, P, I32, P, P, P, ctypes.c_size_t, P]),
     "odba_prefix_chop_f64": (I32, [P, U64, P, P, P, P, I32, P, P, P, ctypes.c_size_t, P]),
     "odba_tune_set": (I32, [I32, I32, I32, I32]),
+    "odba_round_set_bands": (I32, [I32]),
     "odba_tune_query": (I32, [I32, U64, U64, ctypes.c_size_t, P, P]),
     "odba_tune_mode": (None, [I32]),
     "odba_tune_flush": (I32, []),

@@ -440,6 +440,12 @@ int odba_dba_round_ranges_f64(const double *centroid, uint64_t centroid_len, con
                                     stream);
 }
 
+int odba_round_set_bands(int n) {
+  if (n < 0 || n > 8) return fail(ODBA_ERR_INVALID_ARGUMENT, "band count must be 0..8");
+  dba_round_bands(n);
+  return ODBA_OK;
+}
+
 size_t odba_dba_reduce_workspace_bytes(int elem_size, int n) {
   if (n < 1) return 0;
   return elem_size == 8 ? dba_reduce_workspace_bytes<double>(n) : dba_reduce_workspace_bytes<float>(n);

@@ -36,6 +36,9 @@ namespace odba {
 namespace {
 
 constexpr int kRoundWarps = 4;
+constexpr int kReduceThreads = 64;  // centroid indices per block of the ordered reducer
+constexpr int kPlanThreads = 1024;  // members per step of the plan's prefix sums
+constexpr int kRankMembers = 16384;  // longest-first task order computed up to this many members
 // move codes of the reference's path matrix (dtw.hpp:10-16); kMoveDiag,
 // kMoveRight and kMoveUp come with the path sweep (dtw_path.cuh)
 constexpr int kMaxMoveNil = 255, kMoveOpenRight = 4, kMoveNilOpenRight = 5;
@@ -70,6 +73,29 @@ __host__ __device__ inline MemberGeom member_geom(uint64_t len, uint64_t Lc, int
   g.steps = (g.m - g.r0 + 1) / 2 + 31;
   g.words = (unsigned long long)g.swaths * g.steps * 64ull;
   return g;
+}
+
+// Rows of a swath-pipeline task.  With nbands > 1 each member's rows r0 ..
+// m-1 are cut into bands of an even height of at least kMinBandRows (so a
+// band's steps are the whole swath's steps from (rb - r0) / 2 on); count is
+// the member's number of bands, band b covers rows rb .. re-1.
+constexpr int kMinBandRows = 1024;
+struct Band {
+  int rb, re, count;
+};
+__host__ __device__ inline Band member_band(const MemberGeom &g, int nbands, int b) {
+  const int rows = g.m - g.r0;
+  Band o;
+  int h = rows;
+  if (nbands > 1 && rows > 0) {
+    h = (rows + nbands - 1) / nbands;
+    h = (h + 1) & ~1;
+    if (h < kMinBandRows) h = kMinBandRows;
+  }
+  o.count = (rows > 0 && h > 0) ? (rows + h - 1) / h : 1;
+  o.rb = g.r0 + b * h;
+  o.re = b >= o.count - 1 ? g.m : o.rb + h;
+  return o;
 }
 
 // Jobs share one launch: job J owns centroid centroids[coff[J] .. + clen[J]),
@@ -107,9 +133,18 @@ struct RoundArgs {
   // swath pipeline (many warps per member): one progress word and the right
   // edge's minimum and top-row value per (member, swath)
   unsigned long long *prog;
-  T *emtop;
+  T *emtop;  // per (band, member, swath)
   unsigned *err;
   int max_swaths;
+  // row bands of the swath pipeline (member_band): per (member, swath) the
+  // last row and edge corner of the band done so far, and that band's count
+  int nbands = 1;
+  T *rowbuf = nullptr;
+  unsigned long long *bdone = nullptr;
+  // the backtrack's row walk inside the path DTW: a member's last task to
+  // finish walks its path (per member, the count of its tasks done)
+  int walk_in_sweep = 0;
+  unsigned long long *mdone = nullptr;
   T *means;
   uint32_t *counts;
   double *deltas;
@@ -133,24 +168,102 @@ __device__ __forceinline__ MemberGeom geom_of(const RoundArgs<T> &a, int k, int 
 // listing keeps a slot for every member so its layout does not depend on the
 // flags.
 template <typename T>
-__global__ void plan_kernel(RoundArgs<T> a) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned long long w = 0, p = 0, r = 0, rr = 0;
-  for (int k = 0; k < a.nmem; ++k) {
-    int job;
-    const MemberGeom g = geom_of<T>(a, k, job);
-    a.path_off[k] = w;
-    a.trip_off[k] = p;
-    a.rng_off[k] = r;
-    if (a.runs_off) a.runs_off[k] = rr;
-    p += (unsigned long long)(g.m + g.n + 1);
-    if (!(a.jflags[job] & 4)) continue;
-    w += g.words;
-    r += (unsigned long long)a.clen[job];
-    rr += (unsigned long long)g.m;
+__global__ void __launch_bounds__(kPlanThreads) plan_kernel(RoundArgs<T> a) {
+  // exclusive prefix sums over the members, kPlanThreads at a time: path
+  // words, path-listing triples (every member), ranges and rows (active
+  // members only)
+  __shared__ unsigned long long s_warp[4][kPlanThreads / 32];
+  __shared__ unsigned long long s_carry[4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x < 4) s_carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (int base = 0; base < a.nmem; base += kPlanThreads) {
+    const int k = base + threadIdx.x;
+    unsigned long long v[4] = {0ull, 0ull, 0ull, 0ull}, x[4];
+    if (k < a.nmem) {
+      int job;
+      const MemberGeom g = geom_of<T>(a, k, job);
+      v[1] = (unsigned long long)(g.m + g.n + 1);
+      if (a.jflags[job] & 4) {
+        v[0] = g.words;
+        v[2] = (unsigned long long)a.clen[job];
+        v[3] = (unsigned long long)g.m;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      x[q] = v[q];
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, x[q], off);
+        if (lane >= off) x[q] += y;
+      }
+      if (lane == 31) s_warp[q][wid] = x[q];
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const unsigned long long t = lane < kPlanThreads / 32 ? s_warp[q][lane] : 0ull;
+        unsigned long long y = t;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const unsigned long long z = __shfl_up_sync(kFull, y, off);
+          if (lane >= off) y += z;
+        }
+        if (lane < kPlanThreads / 32) s_warp[q][lane] = y - t;  // exclusive over warps
+      }
+    }
+    __syncthreads();
+    unsigned long long ex[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ex[q] = s_carry[q] + s_warp[q][wid] + x[q] - v[q];
+    if (k < a.nmem) {
+      a.path_off[k] = ex[0];
+      a.trip_off[k] = ex[1];
+      a.rng_off[k] = ex[2];
+      if (a.runs_off) a.runs_off[k] = ex[3];
+    }
+    __syncthreads();
+    // the last thread's inclusive sums are the next chunk's carries
+    if (threadIdx.x == kPlanThreads - 1) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s_carry[q] = ex[q] + v[q];
+    }
+    __syncthreads();
   }
-  for (int j = 0; j < a.njobs; ++j)
+  for (int j = threadIdx.x; j < a.njobs; j += kPlanThreads)
     if (a.jflags[j] & 4) a.deltas[j] = 0.0;
+}
+
+// Longest first: member k's place in the swath pipeline's task order is the
+// number of members with more rows, or as many and a lower index (inactive
+// members last).  The last tasks taken, and with the row walk in the sweep
+// the last walks, are then the shortest.  Rows come in tiles of the block's
+// size through shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) rank_members_kernel(RoundArgs<T> a, int *order) {
+  __shared__ int s_rows[256];
+  auto rows_of = [&](int i) {
+    int jb;
+    const MemberGeom g = geom_of<T>(a, i, jb);
+    return (a.jflags[jb] & 4) ? g.m : -1;
+  };
+  const int k = blockIdx.x * 256 + threadIdx.x;
+  const int mine = k < a.nmem ? rows_of(k) : -1;
+  int rank = 0;
+  for (int base = 0; base < a.nmem; base += 256) {
+    const int i = base + threadIdx.x;
+    s_rows[threadIdx.x] = i < a.nmem ? rows_of(i) : -1;
+    __syncthreads();
+    const int lim = a.nmem - base < 256 ? a.nmem - base : 256;
+    for (int u = 0; u < lim; ++u) {
+      const int ri = s_rows[u];
+      rank += int(ri > mine) | int(ri == mine && base + u < k);
+    }
+    __syncthreads();
+  }
+  if (k < a.nmem) order[rank] = k;
 }
 
 __global__ void fill_ranges_kernel(int2 *r, unsigned long long count) {
@@ -245,37 +358,80 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
   }
 }
 
-template <typename T, int R>
-__device__ __forceinline__ void path_pipe_swath(const SwathJob<T> &job, const PathOut &po,
-                                                const PipeGate &gate, T &emin, T &etop) {
-  T col[R];
-  sweep_swath_path<T, R, PipeGate>(job, po, col, emin, etop, TileIn<T>{nullptr, -1}, gate);
+// The open-end shortcut of swath-pipeline member k (the rule of
+// path_dtw_kernel, applied to the per-swath right-edge minima afterwards; a
+// swath's minimum is the least of its bands', its top-row value the top
+// band's, the other bands leaving theirs at big): the first qualifying
+// swath boundary, or 0.
+template <typename T>
+__device__ __forceinline__ int member_shortcut(const RoundArgs<T> &a, int k, const MemberGeom &g,
+                                               int flags) {
+  const int os = flags & 1, oe = (flags >> 1) & 1;
+  constexpr int W = 32 * PathTune<T>::RF;
+  if (!oe || os) return 0;
+  const int nb = member_band(g, a.nbands, 0).count;
+  const unsigned long long layer = (unsigned long long)a.nmem * a.max_swaths;
+  for (int s = 0; s + 1 < g.swaths; ++s) {
+    const int cnext = (s + 1) * W;
+    if (cnext % kRefSwath != 0 || cnext <= g.m || cnext >= g.n) continue;
+    T emin = Num<T>::big(), etop = Num<T>::big();
+    for (int b = 0; b < nb; ++b) {
+      const T *et = a.emtop + ((unsigned long long)b * layer + (unsigned long long)k * a.max_swaths + s) * 2;
+      emin = Num<T>::min2(emin, et[0]);
+      etop = Num<T>::min2(etop, et[1]);
+    }
+    if (etop == emin) return cnext;
+  }
+  return 0;
 }
 
-// Path DTW as the swath pipeline: task k is swath k / nmem of the (k % nmem)-th
-// member in alignment order, so a member's swaths run on different warps at
-// once (few or long members keep the GPU busy); the right edge of swath s goes
-// to buffer s % 2 of the member with one progress word per (member, swath),
-// exactly as in the all-pairs swath pipeline.  Each swath also stores its
-// right edge's minimum and top-row value for the open-end shortcut, which
-// shortcut_kernel resolves afterwards (it never changes a recorded move).
+template <typename T>
+__device__ __forceinline__ bool walk_member_runs(const RoundArgs<T> &a, const MemberGeom &g, int k,
+                                                 int os, int oe, int2 *runs);
+
+template <typename T, int R>
+__device__ __forceinline__ void path_pipe_swath(const SwathJob<T> &job, const PathOut &po,
+                                                BandGate gate, TileIn<T> tile, T &emin,
+                                                T &etop) {
+  T col[R];
+  sweep_swath_path<T, R, BandGate>(job, po, col, emin, etop, tile, gate);
+}
+
+// Path DTW as the swath pipeline: task q is band q / (nmem * max_swaths) of
+// swath (q / nmem) % max_swaths of the (q % nmem)-th member in alignment
+// order, so a member's swaths run on different warps at once (few or long
+// members keep the GPU busy).  The right edge of swath s goes to buffer s % 2
+// of the member with one progress word per (member, swath), as in the
+// all-pairs swath pipeline.  With more than one band (member_band), a band
+// starts from the last row and edge corner the band below left in the
+// (member, swath)'s row buffer, once that band has raised the (member,
+// swath)'s band word; bands only shorten the tasks, so the last wave of
+// warps is shorter, and leave every recorded move as it is.  Each band also
+// stores its right edge's minimum and top-row value for the open-end
+// shortcut, which shortcut_kernel resolves afterwards (it never changes a
+// recorded move).  Every wait is on a task taken earlier from the counter.
 template <typename T, int RF, int RQ>
-__global__ void __launch_bounds__(kRoundWarps * 32) path_pipe_kernel(RoundArgs<T> a) {
+__global__ void __launch_bounds__(kRoundWarps * 32, sizeof(T) == 4 ? 3 : 2) path_pipe_kernel(RoundArgs<T> a) {
   __shared__ __align__(16) T stage_mem[kRoundWarps * kStageElems];
   constexpr int W = 32 * RF;
   const int lane = threadIdx.x & 31;
-  const unsigned long long ntasks = (unsigned long long)a.nmem * a.max_swaths;
+  const unsigned long long layer = (unsigned long long)a.nmem * a.max_swaths;
+  const unsigned long long ntasks = layer * a.nbands;
   for (;;) {
     unsigned long long q = 0;
     if (lane == 0) q = atomicAdd(a.counter, 1ull);
     q = __shfl_sync(kFull, q, 0);
     if (q >= ntasks) break;
-    const int s = int(q / a.nmem), qi = int(q - (unsigned long long)s * a.nmem);
+    const int b = int(q / layer);
+    const unsigned long long ql = q - (unsigned long long)b * layer;
+    const int s = int(ql / a.nmem), qi = int(ql - (unsigned long long)s * a.nmem);
     const int k = a.order ? a.order[qi] : a.nmem - 1 - qi;
     int jb;
     const MemberGeom g = geom_of<T>(a, k, jb);
     const int flags = a.jflags[jb];
     if (!(flags & 4) || s >= g.swaths) continue;
+    const Band bd = member_band(g, a.nbands, b);
+    if (b >= bd.count) continue;
     const int oe = (flags >> 1) & 1;
     const T *seq = a.series + a.offsets[a.mseries[k]];
     const T *cen = a.centroids + a.coff[jb];
@@ -283,39 +439,58 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_pipe_kernel(RoundArgs<T
     T *b1 = b0 + a.edge_stride;
     const int c0 = s * W;
     const bool last = s == g.swaths - 1;
+    const int base = bd.rb - g.r0;  // even: bands keep the step layout
+    const unsigned long long ks = (unsigned long long)k * a.max_swaths + s;
+    T *row = a.rowbuf ? a.rowbuf + ks * (W + 32) : nullptr;
+    TileIn<T> tile{nullptr, g.m - 1};
+    T corner = c0 == 0 ? (g.r0 ? Num<T>::big() : T(0)) : (g.r0 ? T(0) : Num<T>::big());
+    if (b > 0) {
+      // the band below, complete: its last row, and its left edge's value there
+      if (lane == 0) wait_word_at_least(a.bdone + ks, (unsigned long long)b, a.err, kWaitLimitNs);
+      __syncwarp();
+      (void)ld_acquire_gpu(a.bdone + ks);
+      tile.col_init = row;
+      corner = s ? row[W] : Num<T>::big();
+    }
+    if (b + 1 < bd.count) {
+      tile.row_out = row;
+      tile.corner_out = row + W;
+    }
     SwathJob<T> job;
     job.x = g.flip ? cen : seq;
     job.y = g.flip ? seq : cen;
-    job.m = g.m;
+    job.m = bd.re;
     job.n = g.n;
     job.c0 = c0;
-    job.r0 = g.r0;
+    job.r0 = bd.rb;
     job.open_end = oe != 0;
-    job.edge_in = s ? (((s - 1) & 1) ? b1 : b0) : nullptr;
-    job.edge_out = last ? nullptr : ((s & 1) ? b1 : b0);
+    job.edge_in = s ? (((s - 1) & 1) ? b1 : b0) + base : nullptr;
+    job.edge_out = last ? nullptr : ((s & 1) ? b1 : b0) + base;
     job.free_diag0 = c0 > 0 && (c0 % kRefSwath) == 0;
-    job.corner_init = c0 == 0 ? (job.r0 ? Num<T>::big() : T(0)) : (job.r0 ? T(0) : Num<T>::big());
+    job.corner_init = corner;
     job.stage = stage_mem + (threadIdx.x >> 5) * kStageElems;
     PathOut po;
-    po.words = a.words + a.path_off[k] + (unsigned long long)s * g.steps * 64ull;
+    po.words = a.words + a.path_off[k] + (unsigned long long)s * g.steps * 64ull +
+               (unsigned long long)(base / 2) * 64ull;
     po.track_min = true;
     unsigned long long *words = a.prog + (unsigned long long)k * a.max_swaths;
-    PipeGate gate;
-    gate.prog_in = words + (s ? s - 1 : 0);
-    gate.prog_out = words + s;
-    gate.err = a.err;
-    gate.limit_ns = kWaitLimitNs;
-    gate.avail = 0;
+    BandGate gate;
+    gate.g.prog_in = words + (s ? s - 1 : 0);
+    gate.g.prog_out = words + s;
+    gate.g.err = a.err;
+    gate.g.limit_ns = kWaitLimitNs;
+    gate.g.avail = 0;
+    gate.base = base;
     T emin, etop;
     const int width = g.n - c0 < W ? g.n - c0 : W;
     const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
     if (rq >= RF) {
-      path_pipe_swath<T, RF>(job, po, gate, emin, etop);
+      path_pipe_swath<T, RF>(job, po, gate, tile, emin, etop);
     } else {
       switch (rq / RQ) {
-#define ODBA_PPCASE(K)                                                                  \
-  case K:                                                                               \
-    if constexpr (K * RQ < RF) path_pipe_swath<T, K * RQ>(job, po, gate, emin, etop);   \
+#define ODBA_PPCASE(K)                                                                          \
+  case K:                                                                                       \
+    if constexpr (K * RQ < RF) path_pipe_swath<T, K * RQ>(job, po, gate, tile, emin, etop);     \
     break;
         ODBA_PPCASE(1)
         ODBA_PPCASE(2)
@@ -330,15 +505,38 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_pipe_kernel(RoundArgs<T
       }
     }
     if (lane == 0) {
-      T *et = a.emtop + ((unsigned long long)k * a.max_swaths + s) * 2;
+      T *et = a.emtop + ((unsigned long long)b * layer + ks) * 2;
       et[0] = emin;
       et[1] = etop;
+    }
+    if (b + 1 < bd.count) {
+      // the row buffer and corner of every lane, then the band word
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) st_release_gpu(a.bdone + ks, (unsigned long long)(b + 1));
+    }
+    if (a.walk_in_sweep) {
+      // Member k's last task to finish resolves its shortcut and walks its
+      // path (pass 1 of the backtrack) while other warps sweep: every task
+      // makes its moves and edge values visible before it is counted.
+      __threadfence();
+      __syncwarp();
+      unsigned long long n = 0;
+      if (lane == 0) n = atomicAdd(a.mdone + k, 1ull) + 1;
+      n = __shfl_sync(kFull, n, 0);
+      if (n == (unsigned long long)g.swaths * bd.count) {
+        __syncwarp();
+        (void)ld_acquire_gpu(a.mdone + k);  // every lane: after all the member's tasks
+        if (lane == 0) a.shortcut[k] = member_shortcut<T>(a, k, g, flags);
+        __syncwarp();
+        walk_member_runs<T>(a, g, k, flags & 1, oe, a.runs + a.runs_off[k]);
+      }
     }
   }
 }
 
-// The open-end shortcut of the swath pipeline's members (the rule of
-// path_dtw_kernel, applied to the per-swath right-edge minima afterwards).
+// The open-end shortcut of the swath pipeline's members (member_shortcut),
+// when the row walk does not run inside the path DTW.
 template <typename T>
 __global__ void shortcut_kernel(RoundArgs<T> a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -347,20 +545,7 @@ __global__ void shortcut_kernel(RoundArgs<T> a) {
   const MemberGeom g = geom_of<T>(a, k, jb);
   const int flags = a.jflags[jb];
   if (!(flags & 4)) return;
-  const int os = flags & 1, oe = (flags >> 1) & 1;
-  constexpr int W = 32 * PathTune<T>::RF;
-  int shortcut = 0;
-  if (oe && !os) {
-    const T *et = a.emtop + (unsigned long long)k * a.max_swaths * 2;
-    for (int s = 0; s + 1 < g.swaths; ++s) {
-      const int cnext = (s + 1) * W;
-      if (cnext % kRefSwath == 0 && cnext > g.m && cnext < g.n && et[2 * s + 1] == et[2 * s]) {
-        shortcut = cnext;
-        break;
-      }
-    }
-  }
-  a.shortcut[k] = shortcut;
+  a.shortcut[k] = member_shortcut<T>(a, k, g, flags);
 }
 
 // Walks member k's path from its end cell toward (0, 0) with one warp and
@@ -456,51 +641,109 @@ __device__ __forceinline__ bool walk_member_runs(const RoundArgs<T> &a, const Me
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
   const bool lead = lane == 0;
-  const long long max_iters = (long long)g.m + g.n + 64;
-  long long iters = 0;
+  // every window advances the walk by a row or an owner: a bound on windows
+  const long long max_windows = (long long)g.m + g.n + 64;
+  long long windows = 0;
   int r = g.m - 1, c = g.n - 1;
   if (shortcut && c >= shortcut) c = shortcut - 1;  // OPEN_RIGHT from the shortcut's column on
-  int entry = c;                                    // the column the walk entered row r at
+  // the column the walk entered row r at; -1 on the open-end top row, whose
+  // interval is its first cell alone
+  int entry = oe ? -1 : c;
+  // A window: rows top .. top - 31 of one owner lane's columns cbeg .. cbeg +
+  // R - 1 (swath s, owner); lane l holds row top - l's planes, word idx of
+  // the member's path (step t = owner + (row - r0) / 2 of the swath: word
+  // (t * 32 + owner) * 2 + (row - r0) % 2).  The windows below (same owner,
+  // 32 rows = 16 steps down: idx - 1024) and to the left (owner - 1, idx -
+  // 66; or the previous swath's last owner) are loaded with it, so a window
+  // left through its last row or its first column is replaced without
+  // waiting on memory or dividing.
+  const long long swath_words = (long long)g.steps * 64;
+  int s = 0, owner = 0, cbeg = 0, R = RF, top = -1;
+  long long idx = 0, down_idx = 0, left_idx = 0;
+  int ls = 0, lowner = 0, lcbeg = 0, lR = RF;
+  unsigned long long word = 0, down_w = 0, left_w = 0;
+  int j = 0;
   for (;;) {
+    if (c < 0) return false;  // walked off column 0
     if (r == 0) {
       if (lead) runs[0] = os ? make_int2(1, 0) : make_int2(0, c);
       return true;
     }
-    const int s = c / W, c0 = s * W;
-    int R = RF;
-    if (s == g.swaths - 1) {
-      const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
-      R = rq < RF ? rq : RF;
+    if (++windows > max_windows) return false;
+    if (top >= 0 && j >= 0 && r == top - 32) {
+      top -= 32;  // the window below
+      word = down_w;
+      idx = down_idx;
+    } else if (top >= 0 && j < 0 && r > top - 32 && cbeg > 0) {
+      s = ls;  // the window to the left
+      owner = lowner;
+      cbeg = lcbeg;
+      R = lR;
+      word = left_w;
+      idx = left_idx;
+    } else {
+      s = c / W;
+      const int c0 = s * W;
+      R = RF;
+      if (s == g.swaths - 1) {
+        const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
+        R = rq < RF ? rq : RF;
+      }
+      owner = (c - c0) / R;
+      cbeg = c0 + owner * R;
+      top = r;
+      const int rr = top - lane - g.r0;
+      idx = s * swath_words + owner * 66 + (long long)(rr >> 1) * 64 + (rr & 1);
+      word = top - lane >= 1 ? w[idx] : 0ull;
     }
-    const int top = r, owner = (c - c0) / R, cbeg = c0 + owner * R;
-    unsigned long long word = 0;
-    const int my_row = top - lane;
-    if (my_row >= 1) {
-      const int rr = my_row - g.r0;
-      const unsigned long long t = (unsigned long long)owner + (rr >> 1);
-      word = w[(unsigned long long)s * g.steps * 64ull + (t * 32 + owner) * 2 + (rr & 1)];
+    down_idx = idx - 1024;
+    down_w = top - 32 - lane >= 1 ? w[down_idx] : 0ull;
+    if (cbeg > 0) {
+      if (owner > 0) {
+        ls = s;
+        lowner = owner - 1;
+        lcbeg = cbeg - R;
+        lR = R;
+        left_idx = idx - 66;
+      } else {
+        ls = s - 1;
+        lowner = 31;
+        lcbeg = cbeg - RF;
+        lR = RF;
+        left_idx = idx - swath_words + 31 * 66;
+      }
+      left_w = top - lane >= 1 ? w[left_idx] : 0ull;
     }
+    const unsigned dul = unsigned(word) | unsigned(word >> 32), dl = unsigned(word);
+    // j: the walk's column within the window; a row's planes are shuffled
+    // one row ahead, off the chain through j
+    const int lim = top - 32 > 0 ? top - 32 : 0;
+    j = c - cbeg;
+    int2 *rp = runs + r;
+    unsigned du_r = __shfl_sync(kFull, dul, (top - r) & 31);
+    unsigned d_r = __shfl_sync(kFull, dl, (top - r) & 31);
     for (;;) {
-      if (++iters > max_iters) return false;
-      const unsigned long long wv = __shfl_sync(kFull, word, (top - r) & 31);
-      const unsigned below = 0xffffffffu >> (31 - (c - cbeg));
-      const unsigned du = (unsigned(wv) | unsigned(wv >> 32)) & below;
-      if (du == 0) {
+      const int ln = (top - r + 1) & 31;
+      const unsigned du_n = __shfl_sync(kFull, dul, ln);
+      const unsigned d_n = __shfl_sync(kFull, dl, ln);
+      const unsigned x = du_r << (31 - j);  // the row's moves at or left of j, top-aligned
+      if (x == 0) {
         // RIGHT through the owner's first column: on in the owner to the left
-        c = cbeg - 1;
-        if (c < 0) return false;
+        j = -1;
         break;
       }
-      const int jp = 31 - __clz(du);
+      const int jp = j - __clz(x);
       const int cp = cbeg + jp;
-      const bool diag = (unsigned(wv) >> jp) & 1u;
-      if (lead) runs[r] = make_int2(cp, (oe && r == g.m - 1) ? cp : entry);
+      if (lead) *rp = make_int2(cp, cp > entry ? cp : entry);
+      --rp;
       --r;
-      c = diag ? cp - 1 : cp;
-      entry = c;
-      if (c < 0) return false;
-      if (r == 0 || top - r >= 32 || c < cbeg) break;  // row 0, or reload the window
+      j = jp - int((d_r >> jp) & 1u);  // one column left after DIAG
+      entry = cbeg + j;
+      du_r = du_n;
+      d_r = d_n;
+      if ((r <= lim) | (j < 0)) break;  // row 0, or a new window
     }
+    c = cbeg + j;
   }
 }
 
@@ -658,50 +901,84 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 
 // grid: (ceil(max centroid length / 256), jobs)
 template <typename T>
-__global__ void reduce_kernel(RoundArgs<T> a) {
-  __shared__ double smax[256];
+__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(RoundArgs<T> a) {
+  __shared__ double smax[kReduceThreads];
+  // a batch: kBatch members; per member the samples the block's centroid
+  // indices receive (a monotone path gives them as one span), staged in
+  // shared memory when the span has at most kSpan samples
+  constexpr int kBatch = 32, kSpan = 1024 / sizeof(T);
+  __shared__ unsigned long long s_rng[kBatch];
+  __shared__ const T *s_seq[kBatch];
+  __shared__ int s_lo[kBatch], s_hi[kBatch];
+  __shared__ T s_buf[kBatch * kSpan];
   const int jb = blockIdx.y;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int Lc = a.clen[jb];
   const bool live = (a.jflags[jb] & 4) != 0;
-  double dl = 0.0;
-  if (live && t < Lc) {
-    T sum = T(0);
-    uint32_t cnt = 0;
-    // Members in batches of kBatch: every member's range, series start and
-    // first (highest) sample of the batch are loaded before any of them is
-    // added, so their latencies overlap; the additions keep the order of the
-    // single-member loop (members in order, samples from the highest down,
-    // the stripe-mode extra sample last).
-    constexpr int kBatch = 8;
-    const int kb = a.mbeg[jb], ke = a.mend[jb];
-    for (int k0 = kb; k0 < ke; k0 += kBatch) {
-      int2 r[kBatch];
-      const T *sq[kBatch];
-      T first[kBatch];
+  const bool mine = live && t < Lc;
+  T sum = T(0);
+  uint32_t cnt = 0;
+  // The additions keep the order of the single-member loop: members in
+  // order, each member's samples from the highest down, the stripe-mode
+  // extra sample last.  Only the loads are batched: ranges, then the spans
+  // (coalesced, the whole block), then the sums from shared memory.
+  const int kb = a.mbeg[jb], ke = live ? a.mend[jb] : kb;
+  for (int k0 = kb; k0 < ke; k0 += kBatch) {
+    if (threadIdx.x < kBatch) {
+      const int k = k0 + threadIdx.x;
+      s_rng[threadIdx.x] = k < ke ? a.rng_off[k] : 0ull;
+      s_seq[threadIdx.x] = a.series + (k < ke ? a.offsets[a.mseries[k]] : 0);
+      s_lo[threadIdx.x] = INT_MAX;
+      s_hi[threadIdx.x] = -1;
+    }
+    __syncthreads();
+    int2 r[kBatch];
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        const int k = k0 + u;
-        r[u] = k < ke ? a.ranges[a.rng_off[k] + t] : make_int2(1, 0);
-        sq[u] = a.series + (k < ke ? a.offsets[a.mseries[k]] : 0);
+    for (int u = 0; u < kBatch; ++u)
+      r[u] = (mine && k0 + u < ke) ? a.ranges[s_rng[u] + t] : make_int2(1, 0);
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u)
+      if (r[u].y >= r[u].x) {
+        atomicMin(&s_lo[u], r[u].x);
+        atomicMax(&s_hi[u], r[u].y);
       }
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) first[u] = r[u].y >= r[u].x ? sq[u][r[u].y] : T(0);
+    __syncthreads();
+    // asynchronous copies: none waits for another
+    for (int u = 0; u < kBatch; ++u) {
+      const int lo = s_lo[u], n = s_hi[u] - lo + 1;
+      if (n > 0 && n <= kSpan)
+        for (int i = threadIdx.x; i < n; i += kReduceThreads)
+          cp_async_elem(s_buf + u * kSpan + i, s_seq[u] + lo + i, int(sizeof(T)));
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    if (mine) {
 #pragma unroll
       for (int u = 0; u < kBatch; ++u) {
         if (r[u].y < r[u].x) continue;
-        sum = add_rn(sum, first[u]);
-        for (int i = r[u].y - 1; i >= r[u].x; --i) sum = add_rn(sum, sq[u][i]);
+        const int lo = s_lo[u];
+        if (s_hi[u] - lo + 1 <= kSpan) {
+          const T *src = s_buf + u * kSpan;
+          for (int i = r[u].y - lo; i >= r[u].x - lo; --i) sum = add_rn(sum, src[i]);
+        } else {
+          const T *src = s_seq[u];
+          for (int i = r[u].y; i >= r[u].x; --i) sum = add_rn(sum, src[i]);
+        }
         cnt += uint32_t(r[u].y - r[u].x + 1);
         if (a.extra) {
-          const int e = a.extra[a.rng_off[k0 + u] + t];
+          const int e = a.extra[s_rng[u] + t];
           if (e >= 0) {
-            sum = add_rn(sum, sq[u][e]);
+            sum = add_rn(sum, s_seq[u][e]);
             ++cnt;
           }
         }
       }
     }
+    __syncthreads();
+  }
+  double dl = 0.0;
+  if (mine) {
     const T mean = cnt ? div_rn<T>(sum, T(cnt)) : host_default_nan<T>();
     a.means[a.coff[jb] + t] = mean;
     a.counts[a.coff[jb] + t] = cnt;
@@ -758,19 +1035,39 @@ int round_grid() {
 
 struct RoundLayout {
   size_t off_counter, off_path, off_trip, off_rng, off_runoff, off_short, off_single, off_ranges,
-      off_runs, off_edges, off_words, off_prog, off_emtop, total;
+      off_runs, off_edges, off_words, off_prog, off_bdone, off_mdone, off_order, off_emtop,
+      off_rowbuf, total;
   unsigned long long edge_stride;
   int max_swaths;
-  bool pipe;  // path DTW as the swath pipeline (two edge columns per member)
+  int nbands;  // row bands of the swath pipeline
+  bool pipe;   // path DTW as the swath pipeline (two edge columns per member)
 };
 
 constexpr size_t kPipeEdgeBytes = size_t(8) << 30;  // per-member edge columns up to 8 GB
+constexpr int kMaxBands = 8;
+constexpr size_t kMaxRowBufBytes = size_t(256) << 20;
+std::atomic<int> g_round_bands{0};  // odba_round_set_bands (0: chosen per launch)
+
+// Row bands of the swath pipeline for `tasks` (member, swath) tasks on
+// `slots` resident warps: two when the tasks make more than one wave and at
+// most four, one otherwise.  Tasks that fit one wave run at once, and bands
+// would only lengthen each (member, swath)'s chain.  Past one wave, halving
+// the tasks halves the last partial wave; more bands cost more than they
+// save, because a band taken from the counter before the band below it is
+// done holds its warp while it waits (400 members x 6 swaths on 1776 warps:
+// path DTW 7.02 ms with one band, 6.84 with two, 7.56 with three, 8.97 with
+// four; 800 members: 11.42, 10.97 and 11.71 ms).
+int pipe_bands(unsigned long long tasks, size_t slots) {
+  const int forced = g_round_bands.load(std::memory_order_relaxed);
+  if (forced > 0) return forced < kMaxBands ? forced : kMaxBands;
+  return (tasks > slots && tasks <= 4ull * slots) ? 2 : 1;
+}
 
 // Workspace layout for nmem members / njobs jobs with the given totals.
 template <typename T>
 RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
                          unsigned long long ranges, unsigned long long maxm, int max_swaths = 0,
-                         unsigned long long rows = 0) {
+                         unsigned long long rows = 0, unsigned long long tasks = 0) {
   auto up = [](size_t b) { return (b + 255) / 256 * 256; };
   RoundLayout L;
   L.edge_stride = (maxm + 32 + 31) / 32 * 32;
@@ -792,8 +1089,15 @@ RoundLayout round_layout(int nmem, int njobs, unsigned long long words,
   L.off_edges = o; o += up(edge_cols * 2 * L.edge_stride * sizeof(T));
   L.off_words = o; o += up(words * 8);
   const size_t ps = L.pipe ? size_t(nmem) * size_t(max_swaths) : 0;
+  L.nbands = L.pipe ? pipe_bands(tasks, slots) : 1;
+  // row buffers for at most kMaxRowBufBytes (many inactive members: no bands)
+  if (L.nbands > 1 && ps * (32 * PathTune<T>::RF + 32) * sizeof(T) > kMaxRowBufBytes) L.nbands = 1;
   L.off_prog = o; o += up(ps * 8);
-  L.off_emtop = o; o += up(ps * 2 * sizeof(T));
+  L.off_bdone = o; o += up(ps * 8);  // cleared with the progress words
+  L.off_mdone = o; o += L.pipe ? up(size_t(nmem) * 8) : 0;  // likewise
+  L.off_order = o; o += L.pipe ? up(size_t(nmem) * 4) : 0;
+  L.off_emtop = o; o += up(ps * L.nbands * 2 * sizeof(T));
+  L.off_rowbuf = o; o += L.nbands > 1 ? up(ps * (32 * PathTune<T>::RF + 32) * sizeof(T)) : 0;
   L.total = o;
   (void)njobs;
   return L;
@@ -803,11 +1107,12 @@ template <typename T>
 void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint64_t *h_clen,
                  const int *h_flags, unsigned long long &words, unsigned long long &ranges,
                  unsigned long long &maxm, int *max_swaths = nullptr,
-                 unsigned long long *rows = nullptr) {
+                 unsigned long long *rows = nullptr, unsigned long long *tasks = nullptr) {
   words = ranges = 0;
   maxm = 1;
   if (max_swaths) *max_swaths = 1;
   if (rows) *rows = 0;
+  if (tasks) *tasks = 0;
   for (int k = 0; k < nmem; ++k) {
     const int j = h_mjob ? h_mjob[k] : 0;
     const int f = h_flags[j];
@@ -818,13 +1123,15 @@ void host_totals(const uint64_t *h_lens, const int *h_mjob, int nmem, const uint
     if ((unsigned long long)g.m > maxm) maxm = g.m;
     if (max_swaths && g.swaths > *max_swaths) *max_swaths = g.swaths;
     if (rows) *rows += (unsigned long long)g.m;
+    if (tasks) *tasks += (unsigned long long)g.swaths;
   }
 }
 
 // Planning, range clearing and the path DTW of a round (everything before
 // the backtrack).
 template <typename T>
-void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_t stream) {
+void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_t stream,
+                  bool walk_runs = false) {
   a.counter = reinterpret_cast<unsigned long long *>(base + L.off_counter);
   a.path_off = reinterpret_cast<unsigned long long *>(base + L.off_path);
   a.trip_off = reinterpret_cast<unsigned long long *>(base + L.off_trip);
@@ -838,20 +1145,30 @@ void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_
   a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
   a.prog = reinterpret_cast<unsigned long long *>(base + L.off_prog);
   a.emtop = reinterpret_cast<T *>(base + L.off_emtop);
+  a.bdone = reinterpret_cast<unsigned long long *>(base + L.off_bdone);
+  a.rowbuf = L.nbands > 1 ? reinterpret_cast<T *>(base + L.off_rowbuf) : nullptr;
+  a.nbands = L.nbands;
+  a.mdone = reinterpret_cast<unsigned long long *>(base + L.off_mdone);
+  a.walk_in_sweep = (L.pipe && walk_runs) ? 1 : 0;
   a.err = reinterpret_cast<unsigned *>(base + L.off_counter + 8);
   a.max_swaths = L.max_swaths;
   const unsigned long long nr = (L.off_edges - L.off_ranges) / sizeof(int2);
   cudaMemsetAsync(a.counter, 0, 16, stream);  // work counter and error word
-  plan_kernel<T><<<1, 32, 0, stream>>>(a);
+  plan_kernel<T><<<1, kPlanThreads, 0, stream>>>(a);
   fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
   // with fewer members than resident warps, one block per member spreads
   // them over the SMs instead of leaving them to the first blocks placed
   const bool spread = a.nmem < round_grid<T>() * kRoundWarps;
   if (L.pipe) {
-    cudaMemsetAsync(a.prog, 0, size_t(a.nmem) * L.max_swaths * 8, stream);
+    cudaMemsetAsync(a.prog, 0, L.off_order - L.off_prog, stream);  // progress, band, member words
+    if (!a.order && a.nmem <= kRankMembers) {
+      int *ord = reinterpret_cast<int *>(base + L.off_order);
+      rank_members_kernel<T><<<(a.nmem + 255) / 256, 256, 0, stream>>>(a, ord);
+      a.order = ord;
+    }
     path_pipe_kernel<T, PathTune<T>::RF, PathTune<T>::RQ>
         <<<round_grid<T>(), kRoundWarps * 32, 0, stream>>>(a);
-    shortcut_kernel<T><<<(a.nmem + 127) / 128, 128, 0, stream>>>(a);
+    if (!a.walk_in_sweep) shortcut_kernel<T><<<(a.nmem + 127) / 128, 128, 0, stream>>>(a);
   } else if (spread)
     path_dtw_kernel<T, PathTune<T>::RF, PathTune<T>::RQ, 1><<<a.nmem, 32, 0, stream>>>(a);
   else
@@ -860,25 +1177,29 @@ void launch_paths(RoundArgs<T> &a, const RoundLayout &L, char *base, cudaStream_
 }
 
 // The backtrack: with a path listing one kernel walking cell by cell; without,
-// the row walk (pass 1) and the parallel conversion of its row intervals into
-// ranges (pass 2).
+// the row walk (pass 1, inside the swath pipeline's path DTW when it ran
+// there) and the parallel conversion of its row intervals into ranges
+// (pass 2).
 template <typename T>
 void launch_backtrack(const RoundArgs<T> &a, cudaStream_t stream) {
-  backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
+  if (!a.walk_in_sweep)
+    backtrack_kernel<T><<<(a.nmem + kRoundWarps - 1) / kRoundWarps, kRoundWarps * 32, 0, stream>>>(a);
   if (!a.triples) runs_to_ranges_kernel<T><<<a.nmem, 256, 0, stream>>>(a);
 }
 
 template <typename T>
 int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen,
                  cudaStream_t stream) {
-  launch_paths<T>(a, L, base, stream);
+  launch_paths<T>(a, L, base, stream, !a.triples);
   launch_backtrack<T>(a, stream);
-  dim3 rg((max_clen + 255) / 256, a.njobs);
-  reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
+  dim3 rg((max_clen + kReduceThreads - 1) / kReduceThreads, a.njobs);
+  reduce_kernel<T><<<rg, kReduceThreads, 0, stream>>>(a);
   return check_launch("DBA round kernels");
 }
 
 }  // namespace
+
+int dba_round_bands(int n) { return g_round_bands.exchange(n); }
 
 template <typename T>
 size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int os, int oe) {
@@ -886,10 +1207,10 @@ size_t dba_round_workspace_bytes(const uint64_t *h_lens, int n, uint64_t Lc, int
   const uint64_t clen = Lc;
   const int flags = (os ? 1 : 0) | (oe ? 2 : 0) | 4;
   int ms = 1;
-  unsigned long long rows = 0;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms, &rows);
+  unsigned long long rows = 0, tasks = 0;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms, &rows, &tasks);
   if (Lc > maxm) maxm = Lc;
-  return round_layout<T>(n, 1, words, ranges, maxm, ms, rows).total;
+  return round_layout<T>(n, 1, words, ranges, maxm, ms, rows, tasks).total;
 }
 
 namespace {
@@ -935,10 +1256,10 @@ RoundLayout single_job_layout(const uint64_t *h_lens, int n, uint64_t Lc, int fl
   unsigned long long words, ranges, maxm;
   const uint64_t clen = Lc;
   int ms = 1;
-  unsigned long long rows = 0;
-  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms, &rows);
+  unsigned long long rows = 0, tasks = 0;
+  host_totals<T>(h_lens, nullptr, n, &clen, &flags, words, ranges, maxm, &ms, &rows, &tasks);
   if (Lc > maxm) maxm = Lc;
-  return round_layout<T>(n, 1, words, ranges, maxm, ms, rows);
+  return round_layout<T>(n, 1, words, ranges, maxm, ms, rows, tasks);
 }
 
 }  // namespace
@@ -978,7 +1299,7 @@ int dba_round_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
   RoundArgs<T> a = single_job_round<T>(centroid, Lc, series, offsets, lens, n, flags, L, base, stream);
   // the plan clears the job's delta: point it at a spare word of the header
   a.deltas = reinterpret_cast<double *>(base + L.off_counter + 16);
-  launch_paths<T>(a, L, base, stream);
+  launch_paths<T>(a, L, base, stream, true);
   launch_backtrack<T>(a, stream);
   cudaMemcpyAsync(ranges_out, a.ranges, size_t(n) * Lc * sizeof(int2), cudaMemcpyDeviceToDevice, stream);
   return check_launch("DBA round path and backtrack kernels");
@@ -1010,8 +1331,8 @@ int dba_reduce_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
   a.means = mean;
   a.counts = counts;
   a.deltas = delta;
-  plan_kernel<T><<<1, 32, 0, stream>>>(a);
-  reduce_kernel<T><<<dim3(unsigned((Lc + 255) / 256), 1), 256, 0, stream>>>(a);
+  plan_kernel<T><<<1, kPlanThreads, 0, stream>>>(a);
+  reduce_kernel<T><<<dim3(unsigned((Lc + kReduceThreads - 1) / kReduceThreads), 1), kReduceThreads, 0, stream>>>(a);
   return check_launch("DBA reducer kernels");
 }
 
@@ -1020,11 +1341,11 @@ size_t dba_batch_workspace_bytes(const uint64_t *h_mlens, const int *h_mjob, int
                                  const uint64_t *h_clen, const int *h_flags, int njobs) {
   unsigned long long words, ranges, maxm;
   int ms = 1;
-  unsigned long long rows = 0;
-  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms, &rows);
+  unsigned long long rows = 0, tasks = 0;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms, &rows, &tasks);
   for (int j = 0; j < njobs; ++j)
     if (h_clen[j] > maxm) maxm = h_clen[j];
-  return round_layout<T>(nmem, njobs, words, ranges, maxm, ms, rows).total;
+  return round_layout<T>(nmem, njobs, words, ranges, maxm, ms, rows, tasks).total;
 }
 
 template <typename T>
@@ -1038,11 +1359,11 @@ int dba_batch_launch(const T *centroids, const unsigned long long *coff, const i
                      cudaStream_t stream) {
   unsigned long long words, ranges, maxm;
   int ms = 1;
-  unsigned long long rows = 0;
-  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms, &rows);
+  unsigned long long rows = 0, tasks = 0;
+  host_totals<T>(h_mlens, h_mjob, nmem, h_clen, h_flags, words, ranges, maxm, &ms, &rows, &tasks);
   for (int j = 0; j < njobs; ++j)
     if (h_clen[j] > maxm) maxm = h_clen[j];
-  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm, ms, rows);
+  const RoundLayout L = round_layout<T>(nmem, njobs, words, ranges, maxm, ms, rows, tasks);
   if (ws_bytes < L.total) return fail(ODBA_ERR_WORKSPACE_TOO_SMALL, "DBA batch workspace too small");
   RoundArgs<T> a;
   a.centroids = centroids;
@@ -1659,7 +1980,7 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
   a.edge_stride = L.edge_stride;
   a.words = reinterpret_cast<unsigned long long *>(base + L.off_words);
   const unsigned long long nr = (unsigned long long)n * Lc;
-  plan_kernel<T><<<1, 32, 0, stream>>>(a);
+  plan_kernel<T><<<1, kPlanThreads, 0, stream>>>(a);
   fill_ranges_kernel<<<int(nr / 256 + 1 < 4096 ? nr / 256 + 1 : 4096), 256, 0, stream>>>(a.ranges, nr);
   if (extra) cudaMemsetAsync(extra, 0xff, size_t(nr) * 4, stream);
   if (int rc = check_launch("stripe DBA round set-up")) return rc;
@@ -1752,8 +2073,8 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
     }
     if (int rc = check_launch("stripe DBA round member kernels")) return rc;
   }
-  dim3 rg((unsigned(Lc) + 255) / 256, 1);
-  reduce_kernel<T><<<rg, 256, 0, stream>>>(a);
+  dim3 rg((unsigned(Lc) + kReduceThreads - 1) / kReduceThreads, 1);
+  reduce_kernel<T><<<rg, kReduceThreads, 0, stream>>>(a);
   return check_launch("stripe DBA round reduce");
 }
 

@@ -170,6 +170,11 @@ struct TileIn {
   const T *col_init;
   int top_row;
   const T *top_left = nullptr;
+  // a band of a swath handing its last row to the band above: this lane's R
+  // columns at row_out + lane * R, and (with a left edge) the edge's value
+  // on that row, the next band's corner, at corner_out
+  T *row_out = nullptr;
+  T *corner_out = nullptr;
 };
 
 // Sweeps one swath recording moves.  Same wavefront as sweep_swath; in
@@ -385,6 +390,13 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
   }
   for (; t < total; ++t) masked_step(t);
   if (Gate::kActive && lane31 && has_out) gate.publish(rows);
+  if (tile.row_out) {
+    T *dst = tile.row_out + lane * R;
+#pragma unroll
+    for (int j = 0; j < R; ++j) dst[j] = col[j];
+  }
+  // lane 0's last fetch read the left edge's last row (clamped to it)
+  if (tile.corner_out && has_in && lane0) *tile.corner_out = dg;
   edge_min = __shfl_sync(kFull, emin, 31);
   edge_top = __shfl_sync(kFull, etop, 31);
 }

@@ -62,4 +62,35 @@ struct PipeGate {
   __device__ __forceinline__ void publish(int k) { st_release_gpu(prog_out, (unsigned long long)k); }
 };
 
+// The gate of a band of a swath's rows: the band's rows count from base (its
+// first row's offset in the swath), so the progress words keep counting the
+// whole swath's rows whichever band publishes them.
+struct BandGate {
+  static constexpr bool kActive = true;
+  PipeGate g;
+  int base;
+  __device__ __forceinline__ void wait_in(int k) { g.wait_in(base + k); }
+  __device__ __forceinline__ void publish(int k) { g.publish(base + k); }
+};
+
+// Bounded wait (one thread) until *p >= v, with the gate's error rules:
+// false if the limit ran out (the error word is raised) or another waiter
+// raised it.
+__device__ __forceinline__ bool wait_word_at_least(const unsigned long long *p, unsigned long long v,
+                                                   unsigned *err, unsigned long long limit_ns) {
+  unsigned long long t0 = 0;
+  for (unsigned it = 0;; ++it) {
+    if (ld_acquire_gpu(p) >= v) return true;
+    if (*reinterpret_cast<volatile unsigned *>(err)) return false;
+    const unsigned long long now = global_timer_ns();
+    if (it == 0) {
+      t0 = now;
+    } else if (now - t0 > limit_ns) {
+      atomicExch(err, 1u);
+      return false;
+    }
+    __nanosleep(128);
+  }
+}
+
 }  // namespace odba

@@ -81,6 +81,9 @@ int dba_round_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
                             cudaStream_t stream);
 template <typename T>
 size_t dba_reduce_workspace_bytes(int n);
+// Row bands of the round's swath pipeline: n in 1..8 pins the count, 0 lets
+// each launch choose it.  Returns the previous setting.
+int dba_round_bands(int n);
 template <typename T>
 int dba_reduce_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
                              const uint64_t *offsets, const uint64_t *lens, int n, int os, int oe,

@@ -149,3 +149,60 @@ def test_round_split_into_ranges_and_reduce_equals_whole_round(env, sfx, mode):
     mean1, _, delta1 = sharding.dba_round_sharded(c, ds, 0, 1, os_, oe)
     assert np.array_equal(_bits(mean1.cpu().numpy()), _bits(want_mean.cpu().numpy()))
     assert delta1 == want_delta
+
+
+@pytest.mark.parametrize("nb", [2, 3, 8])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("mode", list(MODES))
+def test_round_row_bands_vs_oracle(env, nb, dtype, mode):
+    # the path DTW's rows cut into bands (odba_round_set_bands): bands of at
+    # least 1024 rows, so these members make 1 to 5 bands, last bands of 1, 2,
+    # 4 or 53 rows among them; flipped members (open end, member longer than
+    # the 2500-sample centroid) band the centroid's rows
+    torch, api = env
+    from opendba_b200 import _native
+    lib = _native.lib()
+    rng = np.random.default_rng(4242 + nb + list(MODES).index(mode))
+    os_, oe = MODES[mode]
+    lens = [5, 900, 2047, 2048, 2049, 2050, 3001, 4100, 2600, 1025]
+    members = [np.cumsum(rng.standard_normal(L)).astype(dtype) for L in lens]
+    centroid = np.cumsum(rng.standard_normal(2500)).astype(dtype)
+    w_mean, w_counts, _, w_delta = O.dba_update(centroid, members, os_, oe, fma_mode=1)
+    assert lib.odba_round_set_bands(nb) == 0
+    try:
+        for with_paths in (False, True):
+            mean, counts, delta, paths = _round(env, centroid, members, os_, oe, with_paths)
+            assert np.array_equal(_bits(mean), _bits(w_mean)), with_paths
+            assert np.array_equal(counts.astype(np.uint32), w_counts)
+            assert delta == w_delta
+        for k, seq in enumerate(members):
+            t = O.path_triples(centroid, seq, os_, oe, fma_mode=1)
+            assert np.array_equal(paths[k], t.astype(np.int32)), f"member {k}"
+    finally:
+        lib.odba_round_set_bands(0)
+
+
+@pytest.mark.parametrize("nb", [1, 2, 4])
+def test_round_row_bands_keep_the_open_end_shortcut(env, nb):
+    # a 1500-row member against a long flat centroid: the shortcut's minimum
+    # is the least over both bands of the swath's right edge
+    torch, api = env
+    from opendba_b200 import _native
+    lib = _native.lib()
+    rng = np.random.default_rng(6)
+    centroid = np.concatenate([np.cumsum(rng.standard_normal(1500)), np.zeros(4000)]).astype(np.float32)
+    members = [centroid[:1500] + 0.01 * rng.standard_normal(1500).astype(np.float32),
+               centroid[:1300].copy()]
+    assert lib.odba_round_set_bands(nb) == 0
+    try:
+        mean, counts, delta, paths = _round(env, centroid, members, 0, 1)
+    finally:
+        lib.odba_round_set_bands(0)
+    w_mean, w_counts, _, w_delta = O.dba_update(centroid, members, 0, 1, fma_mode=1)
+    assert np.array_equal(_bits(mean), _bits(w_mean))
+    assert delta == w_delta
+    for k, seq in enumerate(members):
+        t = O.path_triples(centroid, seq, 0, 1, fma_mode=1)
+        assert np.array_equal(paths[k], t.astype(np.int32))
+    assert (paths[0][:, 2] == 4).sum() > 1000  # the shortcut's OPEN_RIGHT run
+

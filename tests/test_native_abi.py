@@ -77,6 +77,26 @@ def test_tuning_table_set_save_load_without_gpu(native, tmp_path):
     lib.odba_tune_set(8, 12, 20, 0)
 
 
+def test_round_band_setting_without_gpu(native):
+    lib = native
+    assert lib.odba_round_set_bands(9) == 1   # invalid argument
+    assert lib.odba_round_set_bands(-1) == 1
+    u64 = ctypes.c_uint64
+    lens = (u64 * 3)(3000, 5000, 8000)
+    auto = lib.odba_dba_round_workspace_bytes(4, lens, 3, 6012, 0, 0)
+    try:
+        assert lib.odba_round_set_bands(1) == 0
+        one = lib.odba_dba_round_workspace_bytes(4, lens, 3, 6012, 0, 0)
+        assert lib.odba_round_set_bands(4) == 0
+        four = lib.odba_dba_round_workspace_bytes(4, lens, 3, 6012, 0, 0)
+    finally:
+        assert lib.odba_round_set_bands(0) == 0
+    # bands add row buffers; 18 (member, swath) tasks fit one wave of warps
+    # and are not banded automatically
+    assert one < four and auto == one
+    assert lib.odba_dba_round_workspace_bytes(4, lens, 3, 6012, 0, 0) == auto
+
+
 def test_stripe_workspace_sizes_without_gpu(native):
     # host-only size queries of the stripe-mode round: an open end adds the
     # per-(member, centroid index) extra samples and, for double (512-column
