@@ -36,7 +36,8 @@ namespace odba {
 namespace {
 
 constexpr int kRoundWarps = 4;
-constexpr int kReduceThreads = 64;  // centroid indices per block of the ordered reducer
+constexpr int kReduceWarps = 4;  // centroid indices per block of the ordered reducer
+constexpr int kReduceThreads = kReduceWarps * 32;
 constexpr int kPlanThreads = 1024;  // members per step of the plan's prefix sums
 constexpr int kRankMembers = 16384;  // longest-first task order computed up to this many members
 // move codes of the reference's path matrix (dtw.hpp:10-16); kMoveDiag,
@@ -902,100 +903,99 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 // grid: (ceil(max centroid length / 256), jobs)
 template <typename T>
 __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(RoundArgs<T> a) {
-  __shared__ double smax[kReduceThreads];
-  // a batch: kBatch members; per member the samples the block's centroid
-  // indices receive (a monotone path gives them as one span), staged in
-  // shared memory when the span has at most kSpan samples
-  constexpr int kBatch = 32, kSpan = 1024 / sizeof(T);
-  __shared__ unsigned long long s_rng[kBatch];
-  __shared__ const T *s_seq[kBatch];
-  __shared__ int s_lo[kBatch], s_hi[kBatch];
-  __shared__ T s_buf[kBatch * kSpan];
+  // One warp per centroid index: the index's sum is a chain of additions in
+  // the reference's order (members in order, each member's samples from the
+  // highest down, the stripe-mode extra sample last), so the warp's lanes
+  // load the samples of consecutive members at once (lane l the l-th group
+  // of kMpl members of a chunk) and lay them out in that order in the warp's
+  // shared-memory buffer; lane 0 then adds the buffer.  Many warps per SM
+  // keep the loads and the chains of different indices in flight together.
+  constexpr int kCap = 8192 / int(sizeof(T));  // samples per warp's buffer
+  constexpr int kMpl = 8;                      // members per lane per chunk
+  __shared__ T s_buf[kReduceWarps][kCap];
+  __shared__ double s_max[kReduceWarps];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int jb = blockIdx.y;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * kReduceWarps + wid;
   const int Lc = a.clen[jb];
   const bool live = (a.jflags[jb] & 4) != 0;
-  const bool mine = live && t < Lc;
-  T sum = T(0);
-  uint32_t cnt = 0;
-  // The additions keep the order of the single-member loop: members in
-  // order, each member's samples from the highest down, the stripe-mode
-  // extra sample last.  Only the loads are batched: ranges, then the spans
-  // (coalesced, the whole block), then the sums from shared memory.
-  const int kb = a.mbeg[jb], ke = live ? a.mend[jb] : kb;
-  for (int k0 = kb; k0 < ke; k0 += kBatch) {
-    if (threadIdx.x < kBatch) {
-      const int k = k0 + threadIdx.x;
-      s_rng[threadIdx.x] = k < ke ? a.rng_off[k] : 0ull;
-      s_seq[threadIdx.x] = a.series + (k < ke ? a.offsets[a.mseries[k]] : 0);
-      s_lo[threadIdx.x] = INT_MAX;
-      s_hi[threadIdx.x] = -1;
-    }
-    __syncthreads();
-    int2 r[kBatch];
-#pragma unroll
-    for (int u = 0; u < kBatch; ++u)
-      r[u] = (mine && k0 + u < ke) ? a.ranges[s_rng[u] + t] : make_int2(1, 0);
-#pragma unroll
-    for (int u = 0; u < kBatch; ++u)
-      if (r[u].y >= r[u].x) {
-        atomicMin(&s_lo[u], r[u].x);
-        atomicMax(&s_hi[u], r[u].y);
-      }
-    __syncthreads();
-    // asynchronous copies: none waits for another
-    for (int u = 0; u < kBatch; ++u) {
-      const int lo = s_lo[u], n = s_hi[u] - lo + 1;
-      if (n > 0 && n <= kSpan)
-        for (int i = threadIdx.x; i < n; i += kReduceThreads)
-          cp_async_elem(s_buf + u * kSpan + i, s_seq[u] + lo + i, int(sizeof(T)));
-    }
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
-    if (mine) {
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        if (r[u].y < r[u].x) continue;
-        const int lo = s_lo[u];
-        if (s_hi[u] - lo + 1 <= kSpan) {
-          const T *src = s_buf + u * kSpan;
-          for (int i = r[u].y - lo; i >= r[u].x - lo; --i) sum = add_rn(sum, src[i]);
-        } else {
-          const T *src = s_seq[u];
-          for (int i = r[u].y; i >= r[u].x; --i) sum = add_rn(sum, src[i]);
-        }
-        cnt += uint32_t(r[u].y - r[u].x + 1);
-        if (a.extra) {
-          const int e = a.extra[s_rng[u] + t];
-          if (e >= 0) {
-            sum = add_rn(sum, s_seq[u][e]);
-            ++cnt;
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
   double dl = 0.0;
-  if (mine) {
-    const T mean = cnt ? div_rn<T>(sum, T(cnt)) : host_default_nan<T>();
-    a.means[a.coff[jb] + t] = mean;
-    a.counts[a.coff[jb] + t] = cnt;
-    const double d = fabs(double(a.centroids[a.coff[jb] + t] - mean));
-    dl = d > 0.0 ? d : 0.0;  // NaN never raises the maximum (dba.hpp:833)
+  if (live && t < Lc) {
+    T sum = T(0);
+    uint32_t cnt = 0;
+    T *buf = s_buf[wid];
+    const int kb = a.mbeg[jb], ke = a.mend[jb];
+    for (int k0 = kb; k0 < ke; k0 += 32 * kMpl) {
+      int2 r[kMpl];
+      int e[kMpl];
+      const T *sq[kMpl];
+      int n_l = 0;
+#pragma unroll
+      for (int u = 0; u < kMpl; ++u) {
+        const int m = k0 + lane * kMpl + u;
+        r[u] = make_int2(1, 0);
+        e[u] = -1;
+        sq[u] = a.series;
+        if (m < ke) {
+          const unsigned long long ro = a.rng_off[m];
+          r[u] = a.ranges[ro + t];
+          sq[u] = a.series + a.offsets[a.mseries[m]];
+          if (a.extra) e[u] = a.extra[ro + t];
+        }
+        if (r[u].y >= r[u].x) n_l += r[u].y - r[u].x + 1 + (e[u] >= 0 ? 1 : 0);
+      }
+      int incl = n_l;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, off);
+        if (lane >= off) incl += y;
+      }
+      const int total = __shfl_sync(kFull, incl, 31);
+      cnt += uint32_t(total);
+      if (total <= kCap) {
+        int p = incl - n_l;
+#pragma unroll
+        for (int u = 0; u < kMpl; ++u) {
+          if (r[u].y < r[u].x) continue;
+          for (int i = r[u].y; i >= r[u].x; --i) buf[p++] = __ldg(sq[u] + i);
+          if (e[u] >= 0) buf[p++] = __ldg(sq[u] + e[u]);
+        }
+        __syncwarp();
+        if (lane == 0)
+          for (int q = 0; q < total; ++q) sum = add_rn(sum, buf[q]);
+        __syncwarp();
+      } else {
+        // more samples than the buffer holds: the lanes add theirs in turn,
+        // each starting from the previous lane's sum
+        for (int L = 0; L < 32; ++L) {
+          if (lane == L) {
+#pragma unroll
+            for (int u = 0; u < kMpl; ++u) {
+              if (r[u].y < r[u].x) continue;
+              for (int i = r[u].y; i >= r[u].x; --i) sum = add_rn(sum, sq[u][i]);
+              if (e[u] >= 0) sum = add_rn(sum, sq[u][e[u]]);
+            }
+          }
+          sum = __shfl_sync(kFull, sum, L);
+        }
+      }
+    }
+    if (lane == 0) {
+      const T mean = cnt ? div_rn<T>(sum, T(cnt)) : host_default_nan<T>();
+      a.means[a.coff[jb] + t] = mean;
+      a.counts[a.coff[jb] + t] = cnt;
+      const double d = fabs(double(a.centroids[a.coff[jb] + t] - mean));
+      dl = d > 0.0 ? d : 0.0;  // NaN never raises the maximum (dba.hpp:833)
+    }
   }
-  smax[threadIdx.x] = dl;
+  if (lane == 0) s_max[wid] = dl;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s && smax[threadIdx.x + s] > smax[threadIdx.x])
-      smax[threadIdx.x] = smax[threadIdx.x + s];
-    __syncthreads();
+  if (threadIdx.x == 0 && live) {
+    double m = s_max[0];
+    for (int q = 1; q < kReduceWarps; ++q) m = s_max[q] > m ? s_max[q] : m;
+    // non-negative doubles order like their bit patterns
+    atomicMax(reinterpret_cast<unsigned long long *>(a.deltas + jb), (unsigned long long)__double_as_longlong(m));
   }
-  // non-negative doubles order like their bit patterns
-  if (threadIdx.x == 0 && live)
-    atomicMax(reinterpret_cast<unsigned long long *>(a.deltas + jb),
-              (unsigned long long)__double_as_longlong(smax[0]));
 }
 
 // One job, members 0..n-1 in order (the single-cluster DBAUpdate call).
@@ -1192,7 +1192,7 @@ int launch_round(RoundArgs<T> &a, const RoundLayout &L, char *base, int max_clen
                  cudaStream_t stream) {
   launch_paths<T>(a, L, base, stream, !a.triples);
   launch_backtrack<T>(a, stream);
-  dim3 rg((max_clen + kReduceThreads - 1) / kReduceThreads, a.njobs);
+  dim3 rg((max_clen + kReduceWarps - 1) / kReduceWarps, a.njobs);
   reduce_kernel<T><<<rg, kReduceThreads, 0, stream>>>(a);
   return check_launch("DBA round kernels");
 }
@@ -1332,7 +1332,7 @@ int dba_reduce_ranges_launch(const T *centroid, uint64_t Lc, const T *series,
   a.counts = counts;
   a.deltas = delta;
   plan_kernel<T><<<1, kPlanThreads, 0, stream>>>(a);
-  reduce_kernel<T><<<dim3(unsigned((Lc + kReduceThreads - 1) / kReduceThreads), 1), kReduceThreads, 0, stream>>>(a);
+  reduce_kernel<T><<<dim3(unsigned((Lc + kReduceWarps - 1) / kReduceWarps), 1), kReduceThreads, 0, stream>>>(a);
   return check_launch("DBA reducer kernels");
 }
 
@@ -2073,7 +2073,7 @@ int dba_round_stripe_launch(const T *centroid, uint64_t Lc, const T *series,
     }
     if (int rc = check_launch("stripe DBA round member kernels")) return rc;
   }
-  dim3 rg((unsigned(Lc) + kReduceThreads - 1) / kReduceThreads, 1);
+  dim3 rg((unsigned(Lc) + kReduceWarps - 1) / kReduceWarps, 1);
   reduce_kernel<T><<<rg, kReduceThreads, 0, stream>>>(a);
   return check_launch("stripe DBA round reduce");
 }

@@ -22,6 +22,22 @@
 
 namespace odba {
 
+// Swath hand-off of the path sweep.  The next swath's warp can run no closer
+// behind this one than the rows it must see published: lane 31 publishes
+// every kPathPublishSteps steps, and lane 0's rows of chunk c + 1 are gated
+// and copied kPathIssueStep steps into chunk c (a chunk is 32 steps), which
+// leaves 32 - kPathIssueStep steps for the copies to land.  A member's
+// swaths form a chain, so the lag per hand-off adds up over its swaths.
+#ifndef ODBA_PATH_PUBLISH_STEPS
+#define ODBA_PATH_PUBLISH_STEPS 16
+#endif
+#ifndef ODBA_PATH_ISSUE_STEP
+#define ODBA_PATH_ISSUE_STEP 24
+#endif
+constexpr int kPathPublishSteps = ODBA_PATH_PUBLISH_STEPS;
+constexpr int kPathIssueStep = ODBA_PATH_ISSUE_STEP;
+static_assert(kPathIssueStep >= 0 && kPathIssueStep < 31, "chunk c + 1 is issued inside chunk c");
+
 // Sets bit J of w if a == b: one compare and one predicated OR of an
 // immediate (no select, no shifted constant in a register).
 template <int J>
@@ -341,17 +357,25 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
     __syncwarp();
     T pxa = T(0), pxb = T(0), pea = T(0), peb = T(0);
     if (lane0) staged(t, pxa, pxb, pea, peb);
+    int issued = cfirst + 1;  // the last chunk copied
     for (; t < steady_end; ++t) {
       T xa = __shfl_up_sync(kFull, xa_cur, 1);
       T xb = __shfl_up_sync(kFull, xb_cur, 1);
       T la = __shfl_up_sync(kFull, a_last, 1);
       T lb = __shfl_up_sync(kFull, col[R - 1], 1);
-      if (((t + 1) & 31) == 0) {
-        const int c1 = (t + 1) >> 5;
-        cp_async_wait_all();
-        gate_chunk(c1 + 1);
+      if ((t & 31) == kPathIssueStep && (t >> 5) + 1 > issued) {
+        // chunk t / 32 + 1 into the slot chunk t / 32 - 1 left (read by
+        // lane 0 before this step; the gate's __syncwarp orders those reads
+        // before the copies)
+        issued = (t >> 5) + 1;
+        gate_chunk(issued);
         __syncwarp();
-        issue_chunk(c1 + 1);
+        issue_chunk(issued);
+      }
+      if (((t + 1) & 31) == 0) {
+        // chunk (t + 1) / 32 landed, for lane 0's read of step t + 1 below
+        cp_async_wait_all();
+        __syncwarp();
       }
       if (lane0) {
         xa = pxa;
@@ -376,7 +400,7 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
           v.x = a_last;
           v.y = col[R - 1];
           *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
-          if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1)
+          if (Gate::kActive && ((t - 31) % kPathPublishSteps) == kPathPublishSteps - 1)
             gate.publish(2 * (t - 31) + 2);
         }
         const int ra = r0 + 2 * (t - 31);
