@@ -124,6 +124,75 @@ __device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, int 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// A lane's column values y[c] of the swath, and the differences x - y[c] of
+// a step's two rows.  For float the values are kept as packed pairs of
+// adjacent columns, and one sub.rn.f32x2 gives the differences of two
+// columns (each half rounds as sub.rn.f32, so the bits are those of x - y).
+// The differences of a row must be asked for in increasing column order, in
+// fully unrolled code (the column index is then a constant).
+template <typename T, int R>
+struct YCols {
+  T v[R];
+  __device__ __forceinline__ void load(const T *y, int c, int n) {
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[j] = (c + j < n) ? y[c + j] : T(0);
+  }
+  __device__ __forceinline__ T get(int j) const { return v[j]; }
+};
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+template <int H>
+__device__ __forceinline__ float half_f32x2(unsigned long long p) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(p));
+  return H ? hi : lo;
+}
+__device__ __forceinline__ unsigned long long sub_f32x2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+template <int R>
+struct YCols<float, R> {
+  static_assert(R % 2 == 0, "columns come in pairs");
+  unsigned long long p[R / 2];
+  __device__ __forceinline__ void load(const float *y, int c, int n) {
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) {
+      const int j = c + 2 * i;
+      p[i] = pack_f32x2(j < n ? y[j] : 0.f, j + 1 < n ? y[j + 1] : 0.f);
+    }
+  }
+  __device__ __forceinline__ float get(int j) const {
+    return (j & 1) ? half_f32x2<1>(p[j / 2]) : half_f32x2<0>(p[j / 2]);
+  }
+};
+
+template <typename T, int R>
+struct RowDiffs {
+  T xa, xb;
+  __device__ __forceinline__ RowDiffs(T a, T b) : xa(a), xb(b) {}
+  __device__ __forceinline__ T a(const YCols<T, R> &y, int j) const { return xa - y.get(j); }
+  __device__ __forceinline__ T b(const YCols<T, R> &y, int j) const { return xb - y.get(j); }
+};
+template <int R>
+struct RowDiffs<float, R> {
+  unsigned long long xa2, xb2, pa = 0, pb = 0;  // pa, pb: the row's current column pair
+  __device__ __forceinline__ RowDiffs(float a, float b)
+      : xa2(pack_f32x2(a, a)), xb2(pack_f32x2(b, b)) {}
+  __device__ __forceinline__ float a(const YCols<float, R> &y, int j) {
+    if ((j & 1) == 0) pa = sub_f32x2(xa2, y.p[j / 2]);
+    return (j & 1) ? half_f32x2<1>(pa) : half_f32x2<0>(pa);
+  }
+  __device__ __forceinline__ float b(const YCols<float, R> &y, int j) {
+    if ((j & 1) == 0) pb = sub_f32x2(xb2, y.p[j / 2]);
+    return (j & 1) ? half_f32x2<1>(pb) : half_f32x2<0>(pb);
+  }
+};
+
 // One cell: the open-end top-row rule when TOP (the right move is free,
 // dtw.hpp:196-200; at a reference swath-left column the diagonal is free too,
 // dtw.hpp:179-185), the White-Neely cost otherwise.
@@ -144,15 +213,16 @@ __device__ __forceinline__ T cell_rule(T d, T up, T diag, T left, bool top, bool
 // [r0, m); with TOP they may also hold the open-end top row (top_a / top_b),
 // without it the caller guarantees they do not (no open end in this sweep).
 template <typename T, int R, bool MASKED, bool TOP = true>
-__device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T xb, T la, T lb,
-                                        T dg, bool act_a, bool act_b, bool top_a, bool top_b,
-                                        bool fd0) {
+__device__ __forceinline__ T step_rows2(T (&col)[R], const YCols<T, R> &yv, T xa, T xb, T la,
+                                        T lb, T dg, bool act_a, bool act_b, bool top_a,
+                                        bool top_b, bool fd0) {
   T a_left = la, a_diag = dg;
   T b_left = lb, b_diag = la;
+  RowDiffs<T, R> df(xa, xb);
 #pragma unroll
   for (int j = 0; j < R; ++j) {
     const T up = col[j];
-    const T da = xa - yv[j];
+    const T da = df.a(yv, j);
     T va;
     if (MASKED && TOP) {
       va = cell_rule<T>(da, up, a_diag, a_left, top_a, j == 0 && fd0);
@@ -165,7 +235,7 @@ __device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T x
     }
     a_diag = up;
     a_left = va;
-    const T db = xb - yv[j];
+    const T db = df.b(yv, j);
     T vb;
     if (MASKED && TOP) {
       vb = cell_rule<T>(db, va, b_diag, b_left, top_b, j == 0 && fd0);
@@ -191,30 +261,31 @@ __device__ __forceinline__ T step_rows2(T (&col)[R], const T (&yv)[R], T xa, T x
 // in the register of its left neighbour and the whole column would rotate back
 // at the end of each step.  Same cells, same arithmetic, same results.
 template <typename T, int R>
-__device__ __forceinline__ T step_rows2_steady(T (&col)[R], const T (&yv)[R], T xa, T xb, T la,
-                                               T lb, T dg) {
+__device__ __forceinline__ T step_rows2_steady(T (&col)[R], const YCols<T, R> &yv, T xa, T xb,
+                                               T la, T lb, T dg) {
   T a_left = la, a_diag = dg;
   T b_left = lb, b_diag = la;
+  RowDiffs<T, R> df(xa, xb);
   T va_prev;
   {
     const T up = col[0];
-    va_prev = Num<T>::cell(xa - yv[0], Num<T>::min3(up, a_diag, a_left));
+    va_prev = Num<T>::cell(df.a(yv, 0), Num<T>::min3(up, a_diag, a_left));
     a_diag = up;
     a_left = va_prev;
   }
 #pragma unroll
   for (int j = 1; j < R; ++j) {
     const T up = col[j];
-    const T va = Num<T>::cell(xa - yv[j], Num<T>::min3(up, a_diag, a_left));
+    const T va = Num<T>::cell(df.a(yv, j), Num<T>::min3(up, a_diag, a_left));
     a_diag = up;
     a_left = va;
-    const T vb = Num<T>::cell(xb - yv[j - 1], Num<T>::min3(va_prev, b_diag, b_left));
+    const T vb = Num<T>::cell(df.b(yv, j - 1), Num<T>::min3(va_prev, b_diag, b_left));
     b_diag = va_prev;
     b_left = vb;
     col[j - 1] = vb;
     va_prev = va;
   }
-  col[R - 1] = Num<T>::cell(xb - yv[R - 1], Num<T>::min3(va_prev, b_diag, b_left));
+  col[R - 1] = Num<T>::cell(df.b(yv, R - 1), Num<T>::min3(va_prev, b_diag, b_left));
   return a_left;
 }
 
@@ -264,12 +335,8 @@ __device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&c
   const int lane = threadIdx.x & 31;
   const int m = job.m;
   const int r0 = job.r0;
-  T yv[R];
-  {
-    const int cl = job.c0 + lane * R;
-#pragma unroll
-    for (int j = 0; j < R; ++j) yv[j] = (cl + j < job.n) ? job.y[cl + j] : T(0);
-  }
+  YCols<T, R> yv;
+  yv.load(job.y, job.c0 + lane * R, job.n);
   // Row r0 - 1 is the boundary: the virtual row above the matrix (absent,
   // "max") or, with open start, the all-zero row 0.
   const T init = r0 ? T(0) : Num<T>::big();

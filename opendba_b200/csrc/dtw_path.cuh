@@ -83,37 +83,40 @@ __device__ __forceinline__ T path_cell(T d, T up, T diag, T left, bool top, bool
 template <typename T, int R, bool MASKED, int J = 0>
 struct PathCols {
   // Column J of one step: the cells of rows a and b.
-  static __device__ __forceinline__ void run(T (&col)[R], const T (&yv)[R], T xa, T xb, T &a_left,
-                                             T &a_diag, T &b_left, T &b_diag, bool act_a,
-                                             bool act_b, bool top_a, bool top_b, bool fd0,
-                                             unsigned &da, unsigned &ua, unsigned &db,
-                                             unsigned &ub) {
+  static __device__ __forceinline__ void run(T (&col)[R], const YCols<T, R> &yv,
+                                             RowDiffs<T, R> &df, T &a_left, T &a_diag, T &b_left,
+                                             T &b_diag, bool act_a, bool act_b, bool top_a,
+                                             bool top_b, bool fd0, unsigned &da, unsigned &ua,
+                                             unsigned &db, unsigned &ub) {
     if constexpr (J < R) {
       const T up = col[J];
-      T va = path_cell<T, MASKED, J>(xa - yv[J], up, a_diag, a_left, top_a, J == 0 && fd0, da, ua);
+      T va = path_cell<T, MASKED, J>(df.a(yv, J), up, a_diag, a_left, top_a,
+                                     J == 0 && fd0, da, ua);
       if (MASKED) va = act_a ? va : up;
       a_diag = up;
       a_left = va;
-      T vb = path_cell<T, MASKED, J>(xb - yv[J], va, b_diag, b_left, top_b, J == 0 && fd0, db, ub);
+      T vb = path_cell<T, MASKED, J>(df.b(yv, J), va, b_diag, b_left, top_b,
+                                     J == 0 && fd0, db, ub);
       if (MASKED) vb = act_b ? vb : va;
       b_diag = va;
       b_left = vb;
       col[J] = vb;
-      PathCols<T, R, MASKED, J + 1>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a,
+      PathCols<T, R, MASKED, J + 1>::run(col, yv, df, a_left, a_diag, b_left, b_diag, act_a,
                                          act_b, top_a, top_b, fd0, da, ua, db, ub);
     }
   }
 };
 
 template <typename T, int R, bool MASKED>
-__device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa, T xb, T la,
+__device__ __forceinline__ T step_rows2_path(T (&col)[R], const YCols<T, R> &yv, T xa, T xb, T la,
                                              T lb, T dg, bool act_a, bool act_b, bool top_a,
                                              bool top_b, bool fd0, unsigned long long &wa,
                                              unsigned long long &wb) {
   T a_left = la, a_diag = dg;
   T b_left = lb, b_diag = la;
   unsigned da = 0u, ua = 0u, db = 0u, ub = 0u;
-  PathCols<T, R, MASKED, 0>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, act_a, act_b,
+  RowDiffs<T, R> df(xa, xb);
+  PathCols<T, R, MASKED, 0>::run(col, yv, df, a_left, a_diag, b_left, b_diag, act_a, act_b,
                                  top_a, top_b, fd0, da, ua, db, ub);
   wa = (unsigned long long)da | ((unsigned long long)ua << 32);
   wb = (unsigned long long)db | ((unsigned long long)ub << 32);
@@ -125,45 +128,47 @@ __device__ __forceinline__ T step_rows2_path(T (&col)[R], const T (&yv)[R], T xa
 // J, so each new col value can take the register of the old one.
 template <typename T, int R, int J>
 struct PathColsSkew {
-  static __device__ __forceinline__ void run(T (&col)[R], const T (&yv)[R], T xa, T xb, T &a_left,
-                                             T &a_diag, T &b_left, T &b_diag, T &va_prev,
-                                             unsigned &da, unsigned &ua, unsigned &db,
-                                             unsigned &ub) {
+  static __device__ __forceinline__ void run(T (&col)[R], const YCols<T, R> &yv,
+                                             RowDiffs<T, R> &df, T &a_left, T &a_diag, T &b_left,
+                                             T &b_diag, T &va_prev, unsigned &da, unsigned &ua,
+                                             unsigned &db, unsigned &ub) {
     if constexpr (J < R) {
       const T up = col[J];
-      const T va = path_cell<T, false, J>(xa - yv[J], up, a_diag, a_left, false, false, da, ua);
+      const T va =
+          path_cell<T, false, J>(df.a(yv, J), up, a_diag, a_left, false, false, da, ua);
       a_diag = up;
       a_left = va;
-      const T vb = path_cell<T, false, J - 1>(xb - yv[J - 1], va_prev, b_diag, b_left, false, false,
-                                              db, ub);
+      const T vb = path_cell<T, false, J - 1>(df.b(yv, J - 1), va_prev, b_diag, b_left,
+                                              false, false, db, ub);
       b_diag = va_prev;
       b_left = vb;
       col[J - 1] = vb;
       va_prev = va;
-      PathColsSkew<T, R, J + 1>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, va_prev, da,
-                                     ua, db, ub);
+      PathColsSkew<T, R, J + 1>::run(col, yv, df, a_left, a_diag, b_left, b_diag, va_prev, da, ua,
+                                     db, ub);
     }
   }
 };
 
 template <typename T, int R>
-__device__ __forceinline__ T step_rows2_path_steady(T (&col)[R], const T (&yv)[R], T xa, T xb,
-                                                    T la, T lb, T dg, unsigned long long &wa,
+__device__ __forceinline__ T step_rows2_path_steady(T (&col)[R], const YCols<T, R> &yv, T xa,
+                                                    T xb, T la, T lb, T dg,
+                                                    unsigned long long &wa,
                                                     unsigned long long &wb) {
   T a_left = la, a_diag = dg;
   T b_left = lb, b_diag = la;
   unsigned da = 0u, ua = 0u, db = 0u, ub = 0u;
+  RowDiffs<T, R> df(xa, xb);
   T va_prev;
   {
     const T up = col[0];
-    va_prev = path_cell<T, false, 0>(xa - yv[0], up, a_diag, a_left, false, false, da, ua);
+    va_prev = path_cell<T, false, 0>(df.a(yv, 0), up, a_diag, a_left, false, false, da, ua);
     a_diag = up;
     a_left = va_prev;
   }
-  PathColsSkew<T, R, 1>::run(col, yv, xa, xb, a_left, a_diag, b_left, b_diag, va_prev, da, ua, db,
-                             ub);
-  col[R - 1] = path_cell<T, false, R - 1>(xb - yv[R - 1], va_prev, b_diag, b_left, false, false,
-                                          db, ub);
+  PathColsSkew<T, R, 1>::run(col, yv, df, a_left, a_diag, b_left, b_diag, va_prev, da, ua, db, ub);
+  col[R - 1] = path_cell<T, false, R - 1>(df.b(yv, R - 1), va_prev, b_diag, b_left, false,
+                                          false, db, ub);
   wa = (unsigned long long)da | ((unsigned long long)ua << 32);
   wb = (unsigned long long)db | ((unsigned long long)ub << 32);
   return a_left;
@@ -205,12 +210,8 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
   const int lane = threadIdx.x & 31;
   const int m = job.m;
   const int r0 = job.r0;
-  T yv[R];
-  {
-    const int cl = job.c0 + lane * R;
-#pragma unroll
-    for (int j = 0; j < R; ++j) yv[j] = (cl + j < job.n) ? job.y[cl + j] : T(0);
-  }
+  YCols<T, R> yv;
+  yv.load(job.y, job.c0 + lane * R, job.n);
   const T init = r0 ? T(0) : Num<T>::big();
   if (tile.col_init) {
     const T *src = tile.col_init + lane * R;
