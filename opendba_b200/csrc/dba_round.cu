@@ -46,14 +46,31 @@ constexpr int kMaxMoveNil = 255, kMoveOpenRight = 4, kMoveNilOpenRight = 5;
 
 template <typename T>
 struct PathTune;
+// RF: registers (columns) per lane of a full swath; the last, partial swath
+// of a member takes a multiple of RQ.  In the full-path round a last swath
+// within PAD registers of RF is swept at RF (the extra columns past the
+// series' end are swept and never walked), so that one loop body, not two of
+// nearly the same size, runs in most warps.
+#ifndef ODBA_PATH_PAD_F32
+#define ODBA_PATH_PAD_F32 4
+#endif
 template <>
 struct PathTune<float> {
-  static constexpr int RF = 32, RQ = 4;
+  static constexpr int RF = 32, RQ = 4, PAD = ODBA_PATH_PAD_F32;
 };
 template <>
 struct PathTune<double> {
-  static constexpr int RF = 16, RQ = 4;
+  static constexpr int RF = 16, RQ = 4, PAD = 0;
 };
+
+// Registers per lane of a full-path swath `width` columns wide (at most
+// 32 * RF).
+template <typename T>
+__host__ __device__ inline int path_regs(int width) {
+  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ;
+  const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
+  return rq >= RF - PathTune<T>::PAD ? RF : rq;
+}
 
 // Geometry of one member's cost matrix, identical on host and device.
 struct MemberGeom {
@@ -325,7 +342,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32) path_dtw_kernel(RoundArgs<T>
       po.track_min = true;
       T emin, etop;
       const int width = g.n - c0 < W ? g.n - c0 : W;
-      const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
+      const int rq = path_regs<T>(width);
       if (rq >= RF) {
         path_swath<T, RF>(job, po, emin, etop);
       } else {
@@ -484,7 +501,7 @@ __global__ void __launch_bounds__(kRoundWarps * 32, sizeof(T) == 4 ? 3 : 2) path
     gate.base = base;
     T emin, etop;
     const int width = g.n - c0 < W ? g.n - c0 : W;
-    const int rq = ((width + 31) / 32 + RQ - 1) / RQ * RQ;
+    const int rq = path_regs<T>(width);
     if (rq >= RF) {
       path_pipe_swath<T, RF>(job, po, gate, tile, emin, etop);
     } else {
@@ -566,7 +583,7 @@ template <typename T, typename Visit>
 __device__ __forceinline__ bool walk_member_path(const RoundArgs<T> &a, const MemberGeom &g, int k,
                                                  int os, int oe, Visit &&visit) {
   const int lane = threadIdx.x & 31;
-  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
+  constexpr int RF = PathTune<T>::RF, W = 32 * RF;
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
   // A path has at most m + n - 1 cells and never leaves the matrix; the checks
@@ -578,10 +595,7 @@ __device__ __forceinline__ bool walk_member_path(const RoundArgs<T> &a, const Me
   for (;;) {
     const int s = c / W, c0 = s * W;
     int R = RF;
-    if (s == g.swaths - 1) {
-      const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
-      R = rq < RF ? rq : RF;
-    }
+    if (s == g.swaths - 1) R = path_regs<T>(g.n - c0);
     const int top = r, owner = (c - c0) / R, cbeg = c0 + owner * R;
     unsigned long long word = 0;
     const int my_row = top - lane;
@@ -638,7 +652,7 @@ template <typename T>
 __device__ __forceinline__ bool walk_member_runs(const RoundArgs<T> &a, const MemberGeom &g, int k,
                                                  int os, int oe, int2 *runs) {
   const int lane = threadIdx.x & 31;
-  constexpr int RF = PathTune<T>::RF, RQ = PathTune<T>::RQ, W = 32 * RF;
+  constexpr int RF = PathTune<T>::RF, W = 32 * RF;
   const unsigned long long *w = a.words + a.path_off[k];
   const int shortcut = a.shortcut[k];
   const bool lead = lane == 0;
@@ -686,10 +700,7 @@ __device__ __forceinline__ bool walk_member_runs(const RoundArgs<T> &a, const Me
       s = c / W;
       const int c0 = s * W;
       R = RF;
-      if (s == g.swaths - 1) {
-        const int rq = ((g.n - c0 + 31) / 32 + RQ - 1) / RQ * RQ;
-        R = rq < RF ? rq : RF;
-      }
+      if (s == g.swaths - 1) R = path_regs<T>(g.n - c0);
       owner = (c - c0) / R;
       cbeg = c0 + owner * R;
       top = r;
