@@ -378,12 +378,20 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
         cp_async_wait_all();
         __syncwarp();
       }
-      if (lane0) {
-        xa = pxa;
-        xb = pxb;
-        la = pea;
-        lb = peb;
-        staged(t + 1, pxa, pxb, pea, peb);
+      {
+        // lane 0 takes the staged inputs of this step and reads the next
+        // step's; every lane reads the same shared words (one broadcast), so
+        // no lane branches
+        T nxa, nxb, nea, neb;
+        staged(t + 1, nxa, nxb, nea, neb);
+        xa = lane0 ? pxa : xa;
+        xb = lane0 ? pxb : xb;
+        la = lane0 ? pea : la;
+        lb = lane0 ? peb : lb;
+        pxa = nxa;
+        pxb = nxb;
+        pea = nea;
+        peb = neb;
       }
       const T diag = dg;
       dg = lb;
@@ -395,19 +403,22 @@ __device__ __forceinline__ void sweep_swath_path(const SwathJob<T> &job, const P
       w.x = wa;
       w.y = wb;
       reinterpret_cast<ulonglong2 *>(po.words)[t * 32 + lane] = w;
-      if (lane31) {
-        if (has_out) {
+      // lane 31's edge rows and shortcut minimum; the conditions on t are
+      // the same in every lane, and the minimum is kept in every lane (only
+      // lane 31's is read)
+      if (has_out) {
+        if (lane31) {
           V2 v;
           v.x = a_last;
           v.y = col[R - 1];
           *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
-          if (Gate::kActive && ((t - 31) % kPathPublishSteps) == kPathPublishSteps - 1)
-            gate.publish(2 * (t - 31) + 2);
         }
-        const int ra = r0 + 2 * (t - 31);
-        if (shortcut_row<T>(ra)) emin = Num<T>::min2(emin, a_last);
-        if (shortcut_row<T>(ra + 1)) emin = Num<T>::min2(emin, col[R - 1]);
+        if (Gate::kActive && ((t - 31) % kPathPublishSteps) == kPathPublishSteps - 1 && lane31)
+          gate.publish(2 * (t - 31) + 2);
       }
+      const int ra = r0 + 2 * (t - 31);
+      if (shortcut_row<T>(ra)) emin = Num<T>::min2(emin, a_last);
+      if (shortcut_row<T>(ra + 1)) emin = Num<T>::min2(emin, col[R - 1]);
     }
     // the next swath reuses the slots: no copy may still be in flight
     cp_async_wait_all();
