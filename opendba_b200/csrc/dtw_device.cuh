@@ -486,12 +486,20 @@ __device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&c
         __syncwarp();
         issue_chunk(c1 + 1);
       }
-      if (lane0) {
-        xa = pxa;
-        xb = pxb;
-        la = pea;
-        lb = peb;
-        staged(t + 1, pxa, pxb, pea, peb);
+      {
+        // lane 0 takes the staged inputs of this step and reads the next
+        // step's; every lane reads the same shared words (one broadcast), so
+        // no lane branches
+        T nxa, nxb, nea, neb;
+        staged(t + 1, nxa, nxb, nea, neb);
+        xa = lane0 ? pxa : xa;
+        xb = lane0 ? pxb : xb;
+        la = lane0 ? pea : la;
+        lb = lane0 ? peb : lb;
+        pxa = nxa;
+        pxb = nxb;
+        pea = nea;
+        peb = neb;
       }
       const T diag = dg;
       dg = lb;
@@ -499,12 +507,15 @@ __device__ __forceinline__ EdgeStat<T> sweep_swath(const SwathJob<T> &job, T (&c
       xa_cur = xa;
       xb_cur = xb;
       if (CKPT) store_ckpt(r0 + 2 * (t - lane));
-      if (lane31 && has_out) {
-        V2 v;
-        v.x = a_last;
-        v.y = col[R - 1];
-        *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
-        if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1) gate.publish(2 * (t - 31) + 2);
+      if (has_out) {
+        if (lane31) {
+          V2 v;
+          v.x = a_last;
+          v.y = col[R - 1];
+          *reinterpret_cast<V2 *>(job.edge_out + 2 * (t - 31)) = v;
+        }
+        if (Gate::kActive && ((t - 31) % kPublishSteps) == kPublishSteps - 1 && lane31)
+          gate.publish(2 * (t - 31) + 2);
       }
       if (track) {
         const int ra = r0 + 2 * (t - 31);
