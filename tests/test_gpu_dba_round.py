@@ -82,6 +82,29 @@ def test_round_random_vs_oracle(env, dtype, mode):
         assert np.array_equal(paths[k], t.astype(np.int32)), f"member {k}"
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("mode", list(MODES))
+def test_round_padded_last_swath_vs_oracle(env, dtype, mode):
+    # last swaths 864-896 columns wide, which the float round sweeps at the
+    # full 32 columns per lane (the extra columns are never walked): the
+    # 1900-sample centroid's (876), and with the open end the flipped
+    # members' (1904: 880, 2940: 892); both walks (ranges, path listing)
+    rng = np.random.default_rng(1900 + list(MODES).index(mode))
+    os_, oe = MODES[mode]
+    lens = [5, 870, 1100, 1900, 1904, 2940, 3000]
+    members = [np.cumsum(rng.standard_normal(L)).astype(dtype) for L in lens]
+    centroid = np.cumsum(rng.standard_normal(1900)).astype(dtype)
+    w_mean, w_counts, _, w_delta = O.dba_update(centroid, members, os_, oe, fma_mode=1)
+    for with_paths in (False, True):
+        mean, counts, delta, paths = _round(env, centroid, members, os_, oe, with_paths)
+        assert np.array_equal(_bits(mean), _bits(w_mean)), with_paths
+        assert np.array_equal(counts.astype(np.uint32), w_counts)
+        assert delta == w_delta
+    for k, seq in enumerate(members):
+        t = O.path_triples(centroid, seq, os_, oe, fma_mode=1)
+        assert np.array_equal(paths[k], t.astype(np.int32)), f"member {k}"
+
+
 @pytest.mark.parametrize("sfx", ["f32", "f64"])
 def test_round_open_end_shortcut_lane_matches_reference_gpu(env, sfx):
     # a 629-row centroid against longer members: the double build's shortcut
