@@ -51,12 +51,9 @@ struct PathTune;
 // within PAD registers of RF is swept at RF (the extra columns past the
 // series' end are swept and never walked), so that one loop body, not two of
 // nearly the same size, runs in most warps.
-#ifndef ODBA_PATH_PAD_F32
-#define ODBA_PATH_PAD_F32 4
-#endif
 template <>
 struct PathTune<float> {
-  static constexpr int RF = 32, RQ = 4, PAD = ODBA_PATH_PAD_F32;
+  static constexpr int RF = 32, RQ = 4, PAD = 4;
 };
 template <>
 struct PathTune<double> {

@@ -28,14 +28,8 @@ namespace odba {
 // and copied kPathIssueStep steps into chunk c (a chunk is 32 steps), which
 // leaves 32 - kPathIssueStep steps for the copies to land.  A member's
 // swaths form a chain, so the lag per hand-off adds up over its swaths.
-#ifndef ODBA_PATH_PUBLISH_STEPS
-#define ODBA_PATH_PUBLISH_STEPS 16
-#endif
-#ifndef ODBA_PATH_ISSUE_STEP
-#define ODBA_PATH_ISSUE_STEP 24
-#endif
-constexpr int kPathPublishSteps = ODBA_PATH_PUBLISH_STEPS;
-constexpr int kPathIssueStep = ODBA_PATH_ISSUE_STEP;
+constexpr int kPathPublishSteps = 16;
+constexpr int kPathIssueStep = 24;
 static_assert(kPathIssueStep >= 0 && kPathIssueStep < 31, "chunk c + 1 is issued inside chunk c");
 
 // Sets bit J of w if a == b: one compare and one predicated OR of an
