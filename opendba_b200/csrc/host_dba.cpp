@@ -397,6 +397,45 @@ int *read_medoid_indices(const std::string &fname, int n, char **names, int *mem
   return medoids;
 }
 
+// pair_dists.txt (dba.hpp:186-216): row s holds the name of series s, s tabs,
+// "\t0" and its distances to the later series, each after a tab; the last
+// line is the last name, n tabs and "0".  Numbers print as the stream's
+// default format prints them (append_stream_value).  Up to 16 threads
+// format the rows (2 M numbers for 2000 series), which are then written in
+// order.
+template <typename T>
+void write_pair_dists(const std::string &path, char **names, int n, const std::vector<T> &dists) {
+  if (n < 1) return;
+  std::vector<std::string> rows(size_t(n) - 1);
+  std::vector<size_t> off(size_t(n), 0);
+  for (int s = 1; s < n; ++s) off[s] = off[s - 1] + size_t(n - s);
+  const unsigned nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned w = 0; w < nthreads; ++w) {
+    pool.emplace_back([&, w]() {
+      for (int s = int(w); s + 1 < n; s += int(nthreads)) {
+        std::string &r = rows[s];
+        r.reserve(size_t(s) + 16 + size_t(n - s) * 10);
+        r += names[s];
+        r.append(size_t(s), '\t');
+        r += "\t0";
+        const T *d = dists.data() + off[s];
+        for (int j = s + 1; j < n; ++j) {
+          r += '\t';
+          odba::append_stream_value(r, d[j - s - 1]);
+        }
+        r += '\n';
+      }
+    });
+  }
+  for (auto &t : pool) t.join();
+  std::ofstream mats(path.c_str(), std::ios::binary);
+  for (const std::string &r : rows) mats.write(r.data(), std::streamsize(r.size()));
+  mats << names[n - 1];
+  for (int pad = 0; pad < n; ++pad) mats << "\t";
+  mats << "0\n";
+}
+
 // Medoid pass on device-resident series: distances, pair_dists.txt, medoid
 // (dba.hpp:170-351 for one cluster).
 template <typename T>
@@ -417,29 +456,7 @@ int *medoid_pass(const T *d_data, const uint64_t *d_offs, const uint64_t *d_lens
     check_cuda(cudaStreamSynchronize(st), "all-pairs DTW");
     check_wait(ws.p, "all-pairs DTW");
   }
-  std::vector<T> sos(n, T(0));
-  T max_distance = T(0);
-  std::ofstream mats((std::string(output_prefix) + ".pair_dists.txt").c_str());
-  size_t off = 0;
-  for (int s = 0; s + 1 < n; ++s) {
-    mats << names[s];
-    for (int pad = 0; pad < s; ++pad) mats << "\t";
-    mats << "\t0";
-    for (int j = s + 1; j < n; ++j) {
-      T d = dists[off + (j - s - 1)];
-      if (max_distance < d) max_distance = d;
-      mats << "\t" << d;
-      d *= d;
-      sos[s] += d;
-      sos[j] += d;
-    }
-    off += n - s - 1;
-    mats << std::endl;
-  }
-  mats << names[n - 1];
-  for (int pad = 0; pad < n; ++pad) mats << "\t";
-  mats << "0" << std::endl;
-  mats.close();
+  write_pair_dists<T>(std::string(output_prefix) + ".pair_dists.txt", names, n, dists);
   // complete linkage, the cut and the per-cluster medoids (dba.hpp:219-343)
   std::vector<int> med(std::max(n, 1), -1);
   int num_clusters = 1;

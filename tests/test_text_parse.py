@@ -90,3 +90,69 @@ def test_random_values_match_stream_extraction(driver, tmp_path):
     fmts = ["%g", "%.9g", "%.17g", "%e", "%.3f", "%.12E", " %g", "%+g", "%g\r", "%g x"]
     lines = [f % x for x in v for f in fmts[:1]] + [fmts[i % len(fmts)] % x for i, x in enumerate(v)]
     _check(driver, tmp_path, lines)
+
+
+# The writers' number formatter (append_stream_value) against the stream's
+# default output (`out << value`, precision 6), which the reference's
+# pair_dists.txt writer uses (dba.hpp:186-216): the same characters for every
+# value, float and double, finite or not.
+FORMAT_DRIVER = r'''
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <random>
+#include <sstream>
+#include <string>
+#include "text_parse.h"
+
+template <typename T> static long check(T v) {
+  std::string got;
+  odba::append_stream_value(got, v);
+  std::ostringstream want;
+  want << v;
+  if (got == want.str()) return 0;
+  std::printf("mismatch [%s] [%s]\n", got.c_str(), want.str().c_str());
+  return 1;
+}
+
+int main() {
+  long bad = 0, n = 0;
+  const double edge[] = {0.0, -0.0, 1.0, -1.0, 0.1, 1e-5, 1e-4, 123456.0, 1234567.0, 999999.5,
+                         9999995.0, 0.000123456, 1e15, 1e16, 1e-300, 5e-324, 2.2250738585072014e-308,
+                         1.7976931348623157e308, 3.4028234663852886e38, 1.1754943508222875e-38,
+                         1.401298464324817e-45, 100000.0, 1e6, 0.5, 2.5e-7,
+                         std::numeric_limits<double>::infinity(), -std::numeric_limits<double>::infinity(),
+                         std::numeric_limits<double>::quiet_NaN(), -std::numeric_limits<double>::quiet_NaN()};
+  for (double e : edge) {
+    bad += check(e) + check(float(e));
+    n += 2;
+  }
+  std::mt19937_64 g(7);
+  std::uniform_real_distribution<double> u(0.0, 400.0);
+  for (int i = 0; i < 400000; ++i) {
+    const uint64_t b = g();
+    double d;
+    std::memcpy(&d, &b, 8);
+    const uint32_t c = uint32_t(b >> 17);
+    float f;
+    std::memcpy(&f, &c, 4);
+    const double r = u(g);
+    bad += check(d) + check(f) + check(r) + check(float(r)) + check(std::sqrt(r));
+    n += 5;
+  }
+  std::printf("%ld values, %ld mismatches\n", n, bad);
+  return bad ? 1 : 0;
+}
+'''
+
+
+def test_number_formatter_matches_stream_output(tmp_path):
+    src = tmp_path / "fmt.cpp"
+    src.write_text(FORMAT_DRIVER)
+    exe = tmp_path / "fmt"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "opendba_b200", "csrc"),
+                    str(src), "-o", str(exe)], check=True)
+    p = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert p.returncode == 0, p.stdout[-3000:]
