@@ -59,6 +59,7 @@ METRIC = "all-vs-all DTW GCUPS (2000×2–8k, fp32); batched/served vs plain, p5
 N_SERIES, LEN_LO, LEN_HI = 2000, 2000, 8000
 SEED = 0x0DBA0002
 SMS, FP32_LANES, OPS_PER_CELL = 148, 128, 5
+MIN_CPU_CELLS = 1.0e11  # the CPU baseline's smallest sample
 SM_MAX_MHZ = 1965.0
 
 
@@ -167,7 +168,9 @@ def cpu_baseline(series, target_secs: float, seed: int = 7):
     dt = time.perf_counter() - t0
     rate = float((lens[rows[probe]] * lens[cols[probe]]).sum()) / max(dt, 1e-6)
     per_pair = float((lens[rows] * lens[cols]).mean())
-    k = int(max(threads, min(npairs, target_secs * rate / per_pair)))
+    # at least MIN_CPU_CELLS cells, whatever the calibration says (it runs one
+    # pair per thread, so it underestimates the rate of a long sample)
+    k = int(max(threads, min(npairs, max(target_secs * rate, MIN_CPU_CELLS) / per_pair)))
     sample = np.sort(rng.choice(npairs, size=k, replace=False))
     cells = float((lens[rows[sample]] * lens[cols[sample]]).sum())
     t0 = time.perf_counter()
