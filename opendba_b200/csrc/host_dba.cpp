@@ -288,9 +288,18 @@ void write_checkpoint(const std::string &fname, const T *c, size_t len) {
     }
     return;
   }
-  f << c[0];
-  for (size_t i = 1; i < len; ++i) f << " " << c[i];
-  f << std::endl;
+  // the stream's default output of each value (append_stream_value), one
+  // write per round instead of one formatted insertion per value
+  std::string line;
+  line.reserve(len * 12 + 1);
+  odba::append_stream_value(line, c[0]);
+  for (size_t i = 1; i < len; ++i) {
+    line += ' ';
+    odba::append_stream_value(line, c[i]);
+  }
+  line += '\n';
+  f.write(line.data(), std::streamsize(line.size()));
+  f.flush();
 }
 
 template <typename T>
